@@ -1,0 +1,403 @@
+"""Benchmark: modular rank of a 16384 x 16384 matrix over p = 2^61 - 1.
+
+Workload (the single large rank configuration): uniform residues in [0, p)
+from SplitMix64(seed 7) with rejection sampling, row-major, generated on the
+device; rank by blocked Gaussian elimination with the tensor-core (INT8-limb
+tcgen05) trailing update when built, else the u64 Barrett one. One step = one
+full rank of the matrix (a pristine device copy is restored into the work
+buffer at the start of every step; the 2 GiB input is larger than L2).
+
+metric value = algorithmic modular multiply-adds per second
+    W = sum_k (n-1-k)(n-1-j_k) over the pivots (k-th pivot in column j_k),
+i.e. the work of the reference's elimination (src/fp.rs:125-255), summed over
+all ranks and divided by the max-over-ranks device time.
+
+--impl reference times the reference algorithm's CPU restatement (the
+oracle, OpenMP over all host threads) on a bounded sample of the same
+workload; the reference itself is Rust and cannot be built here.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "modlin-rs_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+M61 = (1 << 61) - 1
+N = 16384
+METRIC = "Fp rank modmul/s (INT8-limb TC vs u64 Barrett); BM steps/s; bit-exact; 1 B200"
+UNIT = "modMAC/s"
+
+
+def algorithmic_work(n, pcols):
+    return sum((n - 1 - k) * (n - 1 - j) for k, j in enumerate(pcols))
+
+
+def trailing_work(n, pcols, panel=64):
+    """modMACs of the trailing-update launches: per panel with pb pivots,
+    (rows below the panel's pivots) x (columns right of the panel) x pb."""
+    w, r0 = 0, 0
+    pset = sorted(pcols)
+    idx = 0
+    for col in range(0, n, panel):
+        jend = min(col + panel, n)
+        pb = 0
+        while idx < len(pset) and pset[idx] < jend:
+            pb += 1
+            idx += 1
+        if pb and jend < n:
+            w += (n - r0 - pb) * (n - jend) * pb
+        r0 += pb
+        if r0 >= n:
+            break
+    return w
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def int8_peak_tops(torch):
+    """Dense INT8 tensor throughput on this GPU: cuBLASLt int8 GEMM via
+    torch._int_mm (best of 5, 8192^3). None when unavailable."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t().contiguous().t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def cpu_rank_sample(threads=0, target_s=12.0):
+    """The oracle's blocked rank (the reference algorithm, OpenMP over rows)
+    on a uniform matrix over 2^61-1 sized for ~10-30 s of CPU work."""
+    import oracle
+    n0 = 1024
+    m = oracle.gen_uniform(M61, 7, n0 * n0)
+    t0 = time.perf_counter()
+    r, pc = oracle.rank(M61, m, n0, threads=threads, with_pcols=True)
+    dt = time.perf_counter() - t0
+    rate = algorithmic_work(n0, pc) / dt
+    n = n0
+    while n < 8192 and algorithmic_work(2 * n, range(2 * n)) / rate < target_s:
+        n *= 2
+    if n != n0:
+        m = oracle.gen_uniform(M61, 7, n * n)
+        t0 = time.perf_counter()
+        r, pc = oracle.rank(M61, m, n, threads=threads, with_pcols=True)
+        dt = time.perf_counter() - t0
+    w = algorithmic_work(n, pc)
+    return {"value": w / dt, "seconds": dt, "n": n, "rank": r, "work": w}
+
+
+def host_cores():
+    try:
+        import oracle
+        import ctypes
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count()
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    cores = host_cores()
+    samples = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_rank_sample(threads=0, target_s=8.0)
+        if i >= args.warmup:
+            samples.append(s)
+    v = statistics.median([s["value"] for s in samples])
+    n = samples[0]["n"]
+    sample = (f"rank of one uniform {n}x{n} matrix over 2^61-1 per step (W={samples[0]['work']:.4g} modMAC), "
+              f"oracle restatement of src/fp.rs:125-255 with OpenMP over {cores} threads on {cpu_model()}")
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.median([s["seconds"] for s in samples]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"rank {N}x{N} over 2^61-1, uniform SplitMix64(7) residues (bounded CPU sample)",
+                   "n": N, "p": M61},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Rust (no rustc here); the oracle is its C restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "tc"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import modlin
+    from modlin import fp as mfp
+
+    n = args.n
+    kernel = args.kernel
+    if kernel == "auto":
+        try:
+            modlin.rank(M61, np.eye(2, dtype=np.uint64), 2, kernel="tc")
+            kernel = "tc"
+        except modlin.ModlinError:
+            kernel = "plain"
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # Inputs resident in HBM: a pristine copy and a work buffer (2 x 2 GiB).
+    pristine = torch.empty(n * n, dtype=torch.int64, device="cuda")
+    work = torch.empty_like(pristine)
+    modlin.gen.uniform_device(M61, 7 + rank, pristine.data_ptr(), n * n)
+    torch.cuda.synchronize()
+
+    def step(kern, want_pcols=False):
+        work.copy_(pristine)
+        return mfp.rank_device(M61, work.data_ptr(), n, kernel=kern, pivot_cols=want_pcols)
+
+    r, pcols = step(kernel, True)
+    W = algorithmic_work(n, pcols)
+    Wtr = trailing_work(n, pcols)
+    for _ in range(args.warmup):
+        step(kernel)
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = modlin.kernel_launches()
+    trailing_ms = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        ranks = []
+        for _ in range(args.steps):
+            ranks.append(step(kernel))
+            trailing_ms.append(modlin.last_trailing_ms())
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+    launches = modlin.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = W * world / (ms_per_step * 1e-3)
+    assert all(x == r for x in ranks)
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        # The other kernel at the same size (the TC speed-up claim).
+        other = "plain" if kernel == "tc" else None
+        if other:
+            step(other)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step(other)
+            e1.record()
+            torch.cuda.synchronize()
+            extras["plain_modmac_per_s"] = W / (e0.elapsed_time(e1) * 1e-3)
+            extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
+
+    # End to end through the public C ABI with host buffers: pinned host
+    # matrix -> modlin_rank (H2D copy + rank + D2H of the result) each step.
+    host = torch.empty(n * n, dtype=torch.int64, pin_memory=True)
+    host.copy_(pristine)
+    hnp = host.numpy().view(np.uint64)
+    import ctypes
+    from modlin._lib import RankOpts, lib, szt, u64p
+    opts = RankOpts(mfp.KERNELS[kernel], 0)
+    out = szt(0)
+    hp = hnp.ctypes.data_as(u64p)
+
+    def e2e_step():
+        rc = lib().modlin_rank_ex(M61, hp, n, ctypes.byref(opts), ctypes.byref(out), None,
+                                  ctypes.cast(None, modlin._lib.PROGRESS), None)
+        assert rc == 0 and out.value == r
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": W * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": 8,
+           "ms_per_step": e2e_s * 1e3}
+
+    if rank == 0:
+        peaks = measured_peaks()
+        tr_ms = statistics.median(trailing_ms)
+        n_tr = sum(1 for _ in range(0, n, 64)) - 1
+        per_launch_ms = tr_ms / max(n_tr, 1)
+        if kernel == "tc":
+            int8 = int8_peak_tops(torch)
+            if int8:
+                peak, peak_note = int8, "measured: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU"
+            else:
+                peak = 2 * peaks.get("bf16_tflops", 1590.0)
+                peak_note = "2 x measured bf16 dense (MEASURED_PEAKS.json); int8 GEMM unavailable"
+            achieved = Wtr * 64 * 2 / (tr_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None, "kernel": "trailing_tc (tcgen05 kind::i8)",
+                    "peak_source": peak_note,
+                    "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops",
+                    "avg_launch_ms": per_launch_ms}
+        else:
+            peak = peaks.get("hbm_gbs", 6650.0)
+            # Algorithmic bytes of the plain trailing update: C read + write.
+            bytes_tr = 0
+            for k in range(n_tr):
+                rows = n - 64 * (k + 1)
+                bytes_tr += 16 * rows * rows
+            achieved = bytes_tr / (tr_ms * 1e-3) / 1e9
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": "trailing_plain (u64 Barrett, integer pipes)",
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "avg_launch_ms": per_launch_ms,
+                    "int_pipe_modmac_per_s": Wtr / (tr_ms * 1e-3)}
+        cpu = None
+        if not args.no_cpu_baseline:
+            s = cpu_rank_sample(threads=0, target_s=12.0)
+            cpu = {"value": s["value"], "unit": UNIT, "cores": host_cores(), "kind": "port",
+                   "sample": f"oracle rank (src/fp.rs:125-255 restated, OpenMP) of one uniform {s['n']}x{s['n']} "
+                             f"matrix over 2^61-1, {s['seconds']:.1f} s, on {cpu_model()}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 (INT8 limbs on the tensor cores)" if kernel == "tc"
+            else "u64", "data": "synthetic",
+            "config": {"workload": f"single large rank {n}x{n} over p=2^61-1, uniform SplitMix64({7}+rank) "
+                                   "residues, resident in HBM", "n": n, "p": M61, "kernel": kernel,
+                       "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs (2 GiB) larger than L2", "rank": r, "work_modmac": W},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk.summary(), **extras,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+/*
+ * modlin — B200-native modular rank and linear-complexity engine (C ABI).
+ *
+ * Drop-in boundary for the two hot paths of the modlin crate: the rank of an
+ * n x n matrix over F_p by blocked Gaussian elimination and the linear
+ * complexity of a sequence over F_p by Berlekamp-Massey, p prime, p < 2^63.
+ * Every entry point takes plain pointers and sizes; all device memory is
+ * owned by the library. Host matrices and sequences are owned by the caller.
+ * Results are bit-exact: ranks and linear complexities are mathematical
+ * invariants and every kernel computes exact residues.
+ *
+ * Return codes: MODLIN_OK (0) or a negative MODLIN_E* code; no entry point
+ * aborts the process (the reference panics: src/fp.rs:50-51).
+ * Reference citations are file:line inside the modlin crate.
+ */
+#ifndef MODLIN_H
+#define MODLIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Exported symbols keep default visibility even in -fvisibility=hidden builds. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define MODLIN_OK 0
+#define MODLIN_EINVAL_P (-1)   /* p < 2 or p >= 2^63 (src/fp.rs:50-51) */
+#define MODLIN_EINVAL_N (-2)   /* n == 0 or n*n overflows / exceeds the device limit */
+#define MODLIN_EINPUT (-3)     /* an entry is >= p (checked only on request) */
+#define MODLIN_ECUDA (-4)      /* CUDA runtime error */
+#define MODLIN_ENOMEM (-5)     /* device or host allocation failed */
+#define MODLIN_ETIMEOUT (-6)   /* a bounded device-side wait expired */
+#define MODLIN_ENODEV (-7)     /* no CUDA device */
+#define MODLIN_EINVAL_ARG (-8) /* NULL pointer or invalid option */
+
+/* Progress callback: `done` of `total` columns (rank) or steps (linear
+ * complexity); replaces the reference's generic `pl: &mut impl ProgressLog`
+ * (src/fp.rs:125, :260), which has no C form. May be NULL. */
+typedef void (*modlin_progress_fn)(void *ctx, size_t done, size_t total);
+
+/* Human-readable text for a return code. */
+const char *modlin_strerror(int code);
+
+/* ---- Field contract (src/fp.rs:34-114) ---------------------------------- */
+
+typedef struct {
+    uint64_t p;
+    uint64_t mu_lo, mu_hi;  /* mu = floor((2^128 - 1) / p), src/fp.rs:52 */
+    uint64_t safe_batch;    /* products of (p-1)^2 summable in a u128, src/fp.rs:53-59 */
+} modlin_field;
+
+/* Field::new (src/fp.rs:49-61); MODLIN_EINVAL_P unless 2 <= p < 2^63. */
+int modlin_field_new(uint64_t p, modlin_field *f);
+/* Field::reduce (src/fp.rs:65-67). */
+uint64_t modlin_field_reduce(const modlin_field *f, uint64_t x);
+/* Field::reduce_u128 (src/fp.rs:71-79) of hi * 2^64 + lo. */
+uint64_t modlin_field_reduce_u128(const modlin_field *f, uint64_t hi, uint64_t lo);
+/* Field::mul (src/fp.rs:93-95), canonical inputs. */
+uint64_t modlin_field_mul(const modlin_field *f, uint64_t a, uint64_t b);
+
+/* ---- Rank (src/fp.rs:116-255) ------------------------------------------- */
+
+#define MODLIN_RANK_AUTO 0   /* tensor-core trailing update where it pays */
+#define MODLIN_RANK_PLAIN 1  /* u64 Barrett trailing update on the integer pipes */
+#define MODLIN_RANK_TC 2     /* INT8-limb tcgen05 trailing update */
+
+typedef struct {
+    int kernel;       /* MODLIN_RANK_* */
+    int check_input;  /* nonzero: reject entries >= p with MODLIN_EINPUT */
+} modlin_rank_opts;
+
+/* fp::rank (src/fp.rs:125): rank over F_p of the n x n row-major matrix `m`
+ * (host memory, entries in [0, p)). Like the reference, the contents of `m`
+ * afterwards are unspecified (the GPU path leaves them untouched). */
+int modlin_rank(uint64_t p, uint64_t *m, size_t n, size_t *rank_out,
+                modlin_progress_fn cb, void *cb_ctx);
+
+/* modlin_rank with options; `pivot_cols_out` (may be NULL, else room for n
+ * entries) receives the pivot columns in increasing order — the column
+ * profile, an invariant of the matrix. */
+int modlin_rank_ex(uint64_t p, uint64_t *m, size_t n, const modlin_rank_opts *opts,
+                   size_t *rank_out, size_t *pivot_cols_out,
+                   modlin_progress_fn cb, void *cb_ctx);
+
+/* Same on a device-resident matrix (clobbered); `stream` is a cudaStream_t
+ * (NULL = legacy default stream). The call returns when the rank is known. */
+int modlin_rank_device(uint64_t p, uint64_t *d_m, size_t n, const modlin_rank_opts *opts,
+                       size_t *rank_out, size_t *pivot_cols_out, void *stream);
+
+/* ---- Linear complexity (src/fp.rs:257-308) ------------------------------ */
+
+#define MODLIN_LC_AUTO 0      /* block kernel for short, cooperative grid for long */
+#define MODLIN_LC_BLOCK 1     /* one CTA runs the whole sequence (plain form) */
+#define MODLIN_LC_GRID 2      /* persistent cooperative kernel, one grid barrier per step */
+
+typedef struct {
+    int kernel;       /* MODLIN_LC_* */
+    int check_input;
+    int grid_ctas;    /* MODLIN_LC_GRID: CTAs to use (0 = one per SM) */
+} modlin_lc_opts;
+
+/* fp::linear_complexity (src/fp.rs:260): length of the shortest LFSR that
+ * generates s[0..n) (host memory, entries in [0, p)). */
+int modlin_linear_complexity(uint64_t p, const uint64_t *s, size_t n, size_t *lc_out,
+                             modlin_progress_fn cb, void *cb_ctx);
+int modlin_linear_complexity_ex(uint64_t p, const uint64_t *s, size_t n, const modlin_lc_opts *opts,
+                                size_t *lc_out);
+int modlin_linear_complexity_device(uint64_t p, const uint64_t *d_s, size_t n,
+                                    const modlin_lc_opts *opts, size_t *lc_out, void *stream);
+
+/* ---- Batched jobs (the CLI's `reps`, src/main.rs:82 and :152) ----------- */
+
+typedef struct {
+    uint64_t p;
+    const uint64_t *data; /* host, n*n row-major (rank) or n (linear complexity) */
+    size_t n;
+} modlin_job;
+
+/* Ranks of `count` matrices of any sides and primes in one persistent
+ * launch (matrices are copied; the inputs are not modified). */
+int modlin_rank_batch(const modlin_job *jobs, size_t count, size_t *ranks_out);
+/* Linear complexities of `count` sequences in one persistent launch. */
+int modlin_lc_batch(const modlin_job *jobs, size_t count, size_t *lcs_out);
+
+/* Device-resident batch: data[i] are device pointers. */
+int modlin_lc_batch_device(const uint64_t *p, const uint64_t *const *d_data, const size_t *n,
+                           size_t count, size_t *lcs_out, void *stream);
+
+/* ---- p-values (src/stats.rs) -------------------------------------------- */
+
+double modlin_corank_prob(uint64_t p, size_t n, size_t d);          /* src/stats.rs:52-62 */
+double modlin_corank_tail_pvalue(uint64_t p, size_t n, size_t c);   /* src/stats.rs:69-84 */
+double modlin_lc_left_tail_pvalue(uint64_t p, size_t n, size_t ell);/* src/stats.rs:101-126 */
+/* src/stats.rs:129-137: "0", "1" or Rust's `{:?}` rendering; returns the
+ * length written (excluding the NUL). */
+int modlin_pretty_p_value(double p, char *buf, size_t cap);
+
+/* ---- Generators (src/prng.rs) ------------------------------------------- */
+
+#define MODLIN_PRNG_XOROSHIRO128PP 0
+#define MODLIN_PRNG_MIXMAX17 17
+#define MODLIN_PRNG_MIXMAX240 240
+#define MODLIN_PRNG_MIXMAX256 256
+
+typedef struct modlin_prng modlin_prng;
+/* Prng::try_new (src/prng.rs:58, :152): NULL + *err = MODLIN_EINVAL_ARG for
+ * a rejected seed (MIXMAX forbids 0) or an unknown kind. */
+modlin_prng *modlin_prng_new(int kind, uint64_t seed, int *err);
+/* Prng::NAME (src/prng.rs:56, :288, :309, :330). */
+const char *modlin_prng_name(int kind);
+/* count successive next_u64() outputs. */
+void modlin_prng_fill(modlin_prng *g, uint64_t *out, size_t count);
+void modlin_prng_free(modlin_prng *g);
+
+/* ---- Synthetic workloads ------------------------------------------------ */
+
+/* Uniform residues in [0, p): the top bitlen(p-1) bits of successive
+ * SplitMix64 outputs (state initialised to `seed`), rejected while >= p. */
+int modlin_gen_uniform(uint64_t p, uint64_t seed, uint64_t *out, size_t count);
+/* Same, generated on the device (bit-identical to the host stream). */
+int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t *d_out, size_t count, void *stream);
+/* Planted order-L recurrence: a_1..a_L (a_L redrawn while 0) then
+ * s_0..s_{L-1} uniform residues from SplitMix64(seed);
+ * s[i] = sum_{j=1..L} a_j s[i-j] mod p. */
+int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t *out, size_t count);
+/* Field::reduce on the device, in place (src/main.rs:94-104 fill). */
+int modlin_reduce_device(uint64_t p, uint64_t *d_x, size_t count, void *stream);
+
+/* ---- Diagnostics --------------------------------------------------------- */
+
+/* Number of this library's kernel launches since load (for launch-count
+ * claims in measurements). */
+uint64_t modlin_kernel_launches(void);
+/* Milliseconds spent in the trailing-update kernels of the last rank call,
+ * measured with CUDA events on the launching stream (0 if unavailable). */
+double modlin_last_trailing_ms(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

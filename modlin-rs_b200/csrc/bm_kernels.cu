@@ -1,0 +1,350 @@
+// Berlekamp-Massey over F_p on the GPU (src/fp.rs:257-308).
+//
+// The reference keeps c (connection polynomial), b (the polynomial before the
+// last length change) and a scratch t, computes the discrepancy
+// d = s[i] + sum_{j=1..l} c[j] s[i-j] and updates c[m..m+bl) -= (d/bb) b
+// (src/fp.rs:272-306). The GPU kernels run the same steps fraction-free:
+//     c <- bb * c - d * x^m * b,      b <- old c,  bb <- d   (length change)
+// which keeps every c a nonzero scalar multiple of the reference's c, so every
+// discrepancy is zero exactly when the reference's is and l, m, bl evolve
+// identically — the linear complexity is bit-exact — while no modular inverse
+// (a ~120-multiplication Fermat chain) sits on the sequential path.
+//
+// Kernels:
+//  * bm_block_kernel   — one CTA per sequence; the dot product is a warp-
+//                        shuffle tree reduction mod p, the update a strided
+//                        axpy mod p. Plain form: one sequence per launch.
+//  * bm_batch_kernel   — persistent CTAs pulling sequences (longest first)
+//                        from a device queue: thousands of uneven sequences
+//                        and primes in one launch.
+//  * bm_grid_kernel    — one long sequence on a cooperative grid: every CTA
+//                        owns a slice of c in shared memory; per step one
+//                        bounded-spin grid all-reduce of the partial dots.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "bm_kernels.cuh"
+#include "field.cuh"
+
+namespace modlin {
+
+// Per-thread partial dot sum_{j in my indices, j <= l} c[j] * s[i - j].
+template <class F>
+__device__ __forceinline__ uint64_t partial_dot(const F& f, const uint64_t* c, const uint64_t* __restrict__ s, int64_t i,
+                                                int64_t jbeg, int64_t jend_incl, int stride) {
+  const uint64_t sb = f.safe_batch();
+  u128 acc = 0;
+  uint64_t tot = 0, cnt = 0;
+  for (int64_t j = jbeg; j <= jend_incl; j += stride) {
+    acc += (u128)c[j] * s[i - j];
+    if (++cnt == sb) {
+      tot = f.add(tot, f.reduce(acc));
+      acc = 0;
+      cnt = 0;
+    }
+  }
+  return f.add(tot, f.reduce(acc));
+}
+
+template <class F>
+__device__ __forceinline__ uint64_t warp_sum_mod(const F& f, uint64_t v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = f.add(v, __shfl_down_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// One sequence with the whole CTA. c, b, t: n-entry buffers (shared or global
+// memory) owned by this CTA; ws: 2 x 32 partial slots in shared memory.
+template <class F>
+__device__ int64_t bm_block_run(const F& f, const uint64_t* __restrict__ s, int64_t n, uint64_t* c, uint64_t* b,
+                                uint64_t* t, uint64_t (*ws)[32]) {
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
+  for (int64_t j = tid; j < n; j += T) {
+    c[j] = j == 0;
+    b[j] = j == 0;
+  }
+  __syncthreads();
+  int64_t l = 0, m = 1, bl = 1;
+  uint64_t bb = 1;
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t part = partial_dot(f, c, s, i, tid, l, T);
+    part = warp_sum_mod(f, part);
+    if (lane == 0) ws[i & 1][warp] = part;
+    __syncthreads();
+    uint64_t d = 0;
+    for (int w = 0; w < nw; ++w) d = f.add(d, ws[i & 1][w]);
+    if (d == 0) {
+      ++m;
+      continue;
+    }
+    const bool lenchg = 2 * l <= i;
+    int64_t hi = l + 1 > m + bl ? l + 1 : m + bl;
+    if (hi > n) hi = n;
+    for (int64_t j = tid; j < hi; j += T) {
+      const uint64_t old = c[j];
+      const int64_t jb = j - m;
+      const uint64_t bj = (jb >= 0 && jb < bl) ? b[jb] : 0;
+      c[j] = f.sub(f.mul(bb, old), f.mul(d, bj));
+      if (lenchg && j <= l) t[j] = old;
+    }
+    if (lenchg) {
+      uint64_t* tmp = b;
+      b = t;
+      t = tmp;
+      bl = l + 1;
+      bb = d;
+      l = i + 1 - l;
+      m = 1;
+    } else {
+      ++m;
+    }
+    __syncthreads();
+  }
+  return l;
+}
+
+template <class F>
+__device__ __forceinline__ int64_t bm_block_dispatch(const BmJob& job, uint64_t* c, uint64_t* b, uint64_t* t,
+                                                     uint64_t (*ws)[32]) {
+  FieldParams fp{job.p, job.mu_lo, job.mu_hi, job.safe_batch};
+  return bm_block_run(F(fp), job.s, job.n, c, b, t, ws);
+}
+
+// Plain form: one CTA runs one sequence. Buffers in dynamic shared memory
+// when 3n words fit (smem_words >= 3n), else in the global workspace.
+__global__ void bm_block_kernel(BmJob job, uint64_t* gws, int64_t smem_words, int64_t* out) {
+  extern __shared__ __align__(16) uint64_t bm_smem[];
+  __shared__ uint64_t ws[2][32];
+  uint64_t* base = (3 * job.n <= smem_words) ? bm_smem : gws;
+  uint64_t *c = base, *b = base + job.n, *t = base + 2 * job.n;
+  const int64_t l = job.p == kM61 ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
+                                  : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
+  if (threadIdx.x == 0) *out = l;
+}
+
+// Batched form: persistent CTAs take jobs from a device counter; the host
+// orders jobs longest first (LPT). Each CTA has smem_words of dynamic shared
+// memory and a private global slice of gws_words for jobs that do not fit.
+__global__ void bm_batch_kernel(const BmJob* __restrict__ jobs, int64_t count, unsigned long long* next,
+                                uint64_t* gws, int64_t gws_words, int64_t smem_words, int64_t* out) {
+  extern __shared__ __align__(16) uint64_t bm_smem[];
+  __shared__ uint64_t ws[2][32];
+  __shared__ long long sh_job;
+  for (;;) {
+    if (threadIdx.x == 0) sh_job = (long long)atomicAdd(next, 1ULL);
+    __syncthreads();
+    const long long q = sh_job;
+    __syncthreads();
+    if (q >= count) break;
+    const BmJob job = jobs[q];
+    uint64_t* base = (3 * job.n <= smem_words) ? bm_smem : gws + (int64_t)blockIdx.x * gws_words;
+    uint64_t *c = base, *b = base + job.n, *t = base + 2 * job.n;
+    const int64_t l = job.p == kM61 ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
+                                    : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
+    if (threadIdx.x == 0) out[job.slot] = l;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative grid kernel for one long sequence.
+// ---------------------------------------------------------------------------
+struct GridSync {
+  unsigned long long lo[3], hi[3];
+  unsigned int count;
+  int err;
+};
+
+__device__ __forceinline__ unsigned int ld_volatile_u32(const unsigned int* p) {
+  return *(const volatile unsigned int*)p;
+}
+
+template <class F>
+__global__ void bm_grid_kernel(F f, const uint64_t* __restrict__ s, int64_t n, int64_t chunk, uint64_t* bbuf0,
+                               uint64_t* bbuf1, GridSync* gs, long long spin_limit_cycles, int64_t* out) {
+  extern __shared__ __align__(16) uint64_t cs[];  // my slice of c: [lo, lo + chunk)
+  __shared__ uint64_t ws[2][32];
+  __shared__ uint64_t sh_d;
+  __shared__ int sh_err;
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
+  const int64_t lo = (int64_t)blockIdx.x * chunk;
+  const int64_t hi_own = lo + chunk < n ? lo + chunk : n;
+  const unsigned G = gridDim.x;
+  for (int64_t j = lo + tid; j < hi_own; j += T) {
+    cs[j - lo] = j == 0;
+    bbuf0[j] = j == 0;
+  }
+  if (tid == 0) sh_err = 0;
+  // All b initialisations must be visible grid-wide before step 0 reads them.
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    atomicAdd(&gs->count, 1u);
+    const long long t0 = clock64();
+    while (ld_volatile_u32(&gs->count) < G) {
+      if (clock64() - t0 > spin_limit_cycles || *(volatile int*)&gs->err) {
+        atomicExch(&gs->err, 1);
+        sh_err = 1;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (sh_err) return;
+
+  uint64_t* bcur = bbuf0;
+  uint64_t* bnext = bbuf1;
+  int64_t l = 0, m = 1, bl = 1;
+  uint64_t bb = 1;
+  for (int64_t i = 0; i < n; ++i) {
+    // Partial dot over my slice j in [lo, hi_own) with j <= l.
+    const int64_t jl = l < hi_own - 1 ? l : hi_own - 1;
+    uint64_t part = 0;
+    if (lo <= jl) {
+      const uint64_t sb = f.safe_batch();
+      u128 acc = 0;
+      uint64_t cnt = 0;
+      for (int64_t j = lo + tid; j <= jl; j += T) {
+        acc += (u128)cs[j - lo] * s[i - j];
+        if (++cnt == sb) {
+          part = f.add(part, f.reduce(acc));
+          acc = 0;
+          cnt = 0;
+        }
+      }
+      part = f.add(part, f.reduce(acc));
+    }
+    part = warp_sum_mod(f, part);
+    if (lane == 0) ws[i & 1][warp] = part;
+    __syncthreads();
+    if (tid == 0) {
+      uint64_t bp = 0;
+      for (int w = 0; w < nw; ++w) bp = f.add(bp, ws[i & 1][w]);
+      const int slot = (int)(i % 3);
+      atomicAdd(&gs->lo[slot], (unsigned long long)(bp & 0xffffffffULL));
+      atomicAdd(&gs->hi[slot], (unsigned long long)(bp >> 32));
+      __threadfence();
+      atomicAdd(&gs->count, 1u);
+      const unsigned target = (unsigned)(i + 2) * G;
+      const long long t0 = clock64();
+      while (ld_volatile_u32(&gs->count) < target) {
+        if (clock64() - t0 > spin_limit_cycles || *(volatile int*)&gs->err) {
+          atomicExch(&gs->err, 1);
+          sh_err = 1;
+          break;
+        }
+      }
+      __threadfence();
+      const unsigned long long slo = *(volatile unsigned long long*)&gs->lo[slot];
+      const unsigned long long shi = *(volatile unsigned long long*)&gs->hi[slot];
+      sh_d = f.reduce(((u128)shi << 32) + slo);
+      if (blockIdx.x == 0) {
+        const int rs = (int)((i + 2) % 3);
+        gs->lo[rs] = 0;
+        gs->hi[rs] = 0;
+      }
+    }
+    __syncthreads();
+    if (sh_err) return;
+    const uint64_t d = sh_d;
+    if (d == 0) {
+      ++m;
+      continue;
+    }
+    const bool lenchg = 2 * l <= i;
+    int64_t uhi = l + 1 > m + bl ? l + 1 : m + bl;
+    if (uhi > n) uhi = n;
+    const int64_t jhi = uhi < hi_own ? uhi : hi_own;
+    for (int64_t j = lo + tid; j < jhi; j += T) {
+      const uint64_t old = cs[j - lo];
+      const int64_t jb = j - m;
+      const uint64_t bj = (jb >= 0 && jb < bl) ? __ldcg(bcur + jb) : 0;
+      cs[j - lo] = f.sub(f.mul(bb, old), f.mul(d, bj));
+      if (lenchg && j <= l) __stcg(bnext + j, old);
+    }
+    if (lenchg) {
+      uint64_t* tmp = bcur;
+      bcur = bnext;
+      bnext = tmp;
+      bl = l + 1;
+      bb = d;
+      l = i + 1 - l;
+      m = 1;
+    } else {
+      ++m;
+    }
+    // Own-slice writes are re-read by the same thread next step; the next
+    // grid barrier orders the b writes for the other CTAs.
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && tid == 0) *out = l;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+// ---------------------------------------------------------------------------
+cudaError_t launch_bm_block(const BmJob& job, uint64_t* gws, int64_t smem_words, int threads, int64_t* d_out,
+                            cudaStream_t st) {
+  const size_t smem = (3 * job.n <= smem_words) ? (size_t)(3 * job.n) * 8 : 0;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(bm_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  bm_block_kernel<<<1, threads, smem, st>>>(job, gws, smem_words, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long long* d_next, uint64_t* gws,
+                            int64_t gws_words, int64_t smem_words, int blocks, int threads, int64_t* d_out,
+                            cudaStream_t st) {
+  const size_t smem = (size_t)smem_words * 8;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  bm_batch_kernel<<<blocks, threads, smem, st>>>(d_jobs, count, d_next, gws, gws_words, smem_words, d_out);
+  return cudaGetLastError();
+}
+
+int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words) {
+  const size_t smem = (size_t)smem_words * 8;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bm_batch_kernel, threads, smem);
+  return nb;
+}
+
+template <class F>
+static cudaError_t launch_grid_t(const F& f, const uint64_t* s, int64_t n, int ctas, int threads, uint64_t* b0,
+                                 uint64_t* b1, void* gs, long long spin, int64_t* d_out, cudaStream_t st,
+                                 int* ctas_used) {
+  const int64_t chunk = (n + ctas - 1) / ctas;
+  const size_t smem = (size_t)chunk * 8;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(bm_grid_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm_grid_kernel<F>, threads, smem);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (per_sm < 1 || ctas > per_sm * sms) return cudaErrorCooperativeLaunchTooLarge;
+  *ctas_used = ctas;
+  GridSync* g = (GridSync*)gs;
+  F fc = f;
+  const uint64_t* sp = s;
+  int64_t nn = n, ch = chunk;
+  void* args[] = {(void*)&fc, (void*)&sp, (void*)&nn, (void*)&ch, (void*)&b0, (void*)&b1, (void*)&g, (void*)&spin,
+                  (void*)&d_out};
+  return cudaLaunchCooperativeKernel((void*)bm_grid_kernel<F>, dim3(ctas), dim3(threads), args, smem, st);
+}
+
+cudaError_t launch_bm_grid(const FieldParams& fp, const uint64_t* s, int64_t n, int ctas, int threads, uint64_t* b0,
+                           uint64_t* b1, void* gs, long long spin, int64_t* d_out, cudaStream_t st,
+                           int* ctas_used) {
+  if (fp.p == kM61) return launch_grid_t(FpM61(fp), s, n, ctas, threads, b0, b1, gs, spin, d_out, st, ctas_used);
+  return launch_grid_t(FpBarrett(fp), s, n, ctas, threads, b0, b1, gs, spin, d_out, st, ctas_used);
+}
+
+size_t grid_sync_bytes() { return sizeof(GridSync); }
+
+int grid_sync_err_offset() { return (int)offsetof(GridSync, err); }
+
+}  // namespace modlin

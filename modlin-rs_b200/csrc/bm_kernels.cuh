@@ -1,0 +1,32 @@
+// Berlekamp-Massey launchers (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "field.cuh"
+
+namespace modlin {
+
+// One sequence of a batch: field constants inline so a launch mixes primes.
+struct BmJob {
+  uint64_t p, mu_lo, mu_hi, safe_batch;
+  const uint64_t* s;  // device pointer, n residues
+  int64_t n;
+  int64_t slot;       // output index
+};
+
+cudaError_t launch_bm_block(const BmJob& job, uint64_t* gws, int64_t smem_words, int threads, int64_t* d_out,
+                            cudaStream_t st);
+cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long long* d_next, uint64_t* gws,
+                            int64_t gws_words, int64_t smem_words, int blocks, int threads, int64_t* d_out,
+                            cudaStream_t st);
+int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words);
+cudaError_t launch_bm_grid(const FieldParams& fp, const uint64_t* s, int64_t n, int ctas, int threads, uint64_t* b0,
+                           uint64_t* b1, void* gs, long long spin, int64_t* d_out, cudaStream_t st,
+                           int* ctas_used);
+size_t grid_sync_bytes();
+int grid_sync_err_offset();
+
+}  // namespace modlin

@@ -1,0 +1,615 @@
+// The C ABI (include/modlin.h): device context, the rank driver (panel loop),
+// the linear-complexity drivers, batches and the workload generators.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "../../include/modlin.h"
+#include "bm_kernels.cuh"
+#include "field.cuh"
+#include "gen_kernels.cuh"
+#include "rank_kernels.cuh"
+#include "rank_tc.cuh"
+
+namespace modlin {
+
+std::atomic<uint64_t> g_launches{0};
+static double g_last_trailing_ms = 0.0;
+
+// ---------------------------------------------------------------------------
+// Per-device context: one stream, cached workspaces, pinned staging.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+struct Ctx {
+  int device = -1;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  // rank workspaces
+  DevBuf mat, lbuf, ubuf, upanel, gmat, pstate, ispiv, moves;
+  DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
+  PanelState* h_ps = nullptr;
+  int2* h_moves = nullptr;
+  // linear-complexity workspaces
+  DevBuf seq, bmws, bmout, bmsync, bmjobs, bmnext;
+  int64_t* h_out = nullptr;
+  std::vector<cudaEvent_t> ev;
+};
+
+static std::mutex g_ctx_mu;
+static Ctx* g_ctx[64];
+
+static int get_ctx(Ctx** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MODLIN_ENODEV;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MODLIN_ENODEV;
+  if (dev < 0 || dev >= 64) return MODLIN_ENODEV;
+  std::lock_guard<std::mutex> g(g_ctx_mu);
+  if (!g_ctx[dev]) {
+    Ctx* c = new Ctx();
+    c->device = dev;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return MODLIN_ECUDA;
+    }
+    if (cudaMallocHost((void**)&c->h_ps, sizeof(PanelState)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_moves, sizeof(int2) * kPanel) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_out, sizeof(int64_t) * 4) != cudaSuccess) {
+      delete c;
+      return MODLIN_ENOMEM;
+    }
+    g_ctx[dev] = c;
+  }
+  *out = g_ctx[dev];
+  return MODLIN_OK;
+}
+
+static int cuda_rc(cudaError_t e) {
+  if (e == cudaSuccess) return MODLIN_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return MODLIN_ENOMEM;
+  }
+  return MODLIN_ECUDA;
+}
+
+#define CK(expr)                          \
+  do {                                    \
+    cudaError_t _e = (expr);              \
+    if (_e != cudaSuccess) return cuda_rc(_e); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Rank driver.
+// ---------------------------------------------------------------------------
+struct RankRun {
+  const FieldParams* fp;
+  uint64_t* m;
+  int n;
+  int kernel;
+  cudaStream_t st;
+  Ctx* ctx;
+  std::vector<int>* pcols;
+  modlin_progress_fn cb;
+  void* cb_ctx;
+};
+
+static bool use_tc(const RankRun& R) {
+  if (R.kernel == MODLIN_RANK_PLAIN) return false;
+  if (R.kernel == MODLIN_RANK_TC) return true;
+  return R.n >= tc_crossover_n(R.fp->p);
+}
+
+template <class F>
+static int rank_impl(const RankRun& R, size_t* rank_out) {
+  const F f(*R.fp);
+  Ctx* C = R.ctx;
+  const int n = R.n;
+  const int64_t ld = n;
+  cudaStream_t st = R.st;
+  CK(C->lbuf.ensure((size_t)n * kPanel * 8));
+  CK(C->ubuf.ensure((size_t)kPanel * n * 8));
+  CK(C->upanel.ensure((size_t)kPanel * kPanel * 8));
+  CK(C->gmat.ensure((size_t)kPanel * kPanel * 8));
+  CK(C->pstate.ensure(sizeof(PanelState)));
+  CK(C->ispiv.ensure((size_t)n));
+  CK(C->moves.ensure(sizeof(int2) * kPanel));
+  const bool tc = use_tc(R);
+  if (tc) {
+    CK(C->tcA.ensure(tc_a_bytes(n)));
+    CK(C->tcB.ensure(tc_b_bytes(n)));
+  }
+  uint64_t* Lbuf = C->lbuf.as<uint64_t>();
+  uint64_t* Ubuf = C->ubuf.as<uint64_t>();
+  uint64_t* Upanel = C->upanel.as<uint64_t>();
+  uint64_t* G = C->gmat.as<uint64_t>();
+  PanelState* ps = C->pstate.as<PanelState>();
+  uint8_t* ispiv = C->ispiv.as<uint8_t>();
+  int2* d_moves = C->moves.as<int2>();
+  CK(cudaMemsetAsync(ispiv, 0, (size_t)n, st));
+  g_launches++;
+
+  // Trailing-update timing with events on the launching stream.
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tev;
+  size_t ev_used = 0;
+  auto take_events = [&]() -> std::pair<cudaEvent_t, cudaEvent_t> {
+    while (C->ev.size() < 2 * (ev_used + 1)) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      C->ev.push_back(e);
+    }
+    auto pr = std::make_pair(C->ev[2 * ev_used], C->ev[2 * ev_used + 1]);
+    ++ev_used;
+    return pr;
+  };
+
+  int rank = 0, col = 0;
+  while (col < n && rank < n) {
+    const int jend = std::min(col + kPanel, n);
+    const int W = jend - col;
+    const int r0 = rank;
+    CK(cudaMemsetAsync(ps, 0, sizeof(PanelState), st));
+    g_launches++;
+    int round = 0, pb_lo = 0;
+    PanelState* h = C->h_ps;
+    for (;;) {
+      launch_window<F>(f, R.m, ld, n, r0, col, W, round, ps, Upanel, G, Lbuf, ispiv, st);
+      launch_bulk<F>(f, R.m, ld, n, r0, col, W, pb_lo, ps, Upanel, Lbuf, ispiv, C->num_sms, st);
+      g_launches += 2;
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(h, ps, sizeof(PanelState), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (h->ncand == 0) break;
+      if (h->pb >= W || ++round > kPanel + 1) {
+        // A residual with every panel column pivoted is impossible; report
+        // it instead of looping.
+        return MODLIN_ECUDA;
+      }
+      pb_lo = h->pb;
+    }
+    const int pb = h->pb;
+    for (int k = 0; k < pb; ++k)
+      if (R.pcols) R.pcols->push_back(h->pcol[k]);
+    if (pb > 0 && jend < n) {
+      launch_couple<F>(f, R.m, ld, n, jend, ps, G, Ubuf, n, st);
+      g_launches++;
+      // Compaction: pivot rows leave [r0 + pb, n).
+      std::vector<char> piv_in_top(pb, 0);
+      std::vector<int> holes;
+      for (int k = 0; k < pb; ++k) {
+        const int r = h->prow[k];
+        if (r >= r0 + pb)
+          holes.push_back(r);
+        else
+          piv_in_top[r - r0] = 1;
+      }
+      int nm = 0;
+      for (int t = 0, hi = 0; t < pb; ++t)
+        if (!piv_in_top[t]) C->h_moves[nm++] = make_int2(r0 + t, holes[hi++]);
+      if (nm > 0) {
+        CK(cudaMemcpyAsync(d_moves, C->h_moves, sizeof(int2) * nm, cudaMemcpyHostToDevice, st));
+        launch_moves(R.m, ld, n, jend, d_moves, nm, Lbuf, r0, pb, st);
+        g_launches++;
+      }
+      auto evp = take_events();
+      cudaEventRecord(evp.first, st);
+      if (tc) {
+        CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, Lbuf, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
+                              C->tcB.as<uint8_t>(), C->num_sms, st));
+        g_launches += 3;
+      } else {
+        launch_trailing_plain<F>(f, R.m, ld, r0 + pb, n, jend, Lbuf, r0, Ubuf, n, pb, st);
+        g_launches++;
+      }
+      cudaEventRecord(evp.second, st);
+      CK(cudaGetLastError());
+    }
+    if (pb > 0) {
+      launch_clear_flags(ps, ispiv, st);
+      g_launches++;
+    }
+    rank += pb;
+    col = jend;
+    if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
+  }
+  CK(cudaStreamSynchronize(st));
+  double tms = 0;
+  for (size_t i = 0; i < ev_used; ++i) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, C->ev[2 * i], C->ev[2 * i + 1]) == cudaSuccess) tms += ms;
+  }
+  g_last_trailing_ms = tms;
+  *rank_out = (size_t)rank;
+  return MODLIN_OK;
+}
+
+static int rank_device_locked(Ctx* C, uint64_t p, uint64_t* d_m, size_t n, const modlin_rank_opts* opts,
+                              size_t* rank_out, size_t* pivot_cols_out, cudaStream_t st, modlin_progress_fn cb,
+                              void* cb_ctx) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (n == 0 || n > 0x7fffffff / 2) return MODLIN_EINVAL_N;
+  if (!rank_out) return MODLIN_EINVAL_ARG;
+  std::vector<int> pc;
+  RankRun R{&fp, d_m, (int)n, opts ? opts->kernel : MODLIN_RANK_AUTO, st, C, pivot_cols_out ? &pc : nullptr,
+            cb, cb_ctx};
+  const int rc = p == kM61 ? rank_impl<FpM61>(R, rank_out) : rank_impl<FpBarrett>(R, rank_out);
+  if (rc != MODLIN_OK) return rc;
+  if (pivot_cols_out) {
+    std::sort(pc.begin(), pc.end());
+    for (size_t i = 0; i < pc.size(); ++i) pivot_cols_out[i] = (size_t)pc[i];
+  }
+  return MODLIN_OK;
+}
+
+static bool check_residues(uint64_t p, const uint64_t* x, size_t count) {
+  for (size_t i = 0; i < count; ++i)
+    if (x[i] >= p) return false;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Linear-complexity drivers.
+// ---------------------------------------------------------------------------
+static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, const modlin_lc_opts* opts,
+                            size_t* lc_out, cudaStream_t st) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!lc_out) return MODLIN_EINVAL_ARG;
+  if (n == 0) {
+    *lc_out = 0;
+    return MODLIN_OK;
+  }
+  int kernel = opts ? opts->kernel : MODLIN_LC_AUTO;
+  if (kernel == MODLIN_LC_AUTO) kernel = n >= 16384 ? MODLIN_LC_GRID : MODLIN_LC_BLOCK;
+  CK(C->bmout.ensure(sizeof(int64_t) * 4));
+  int64_t* d_out = C->bmout.as<int64_t>();
+  if (kernel == MODLIN_LC_BLOCK) {
+    const int64_t smem_words = (200 * 1024) / 8;
+    if (3 * (int64_t)n > smem_words) CK(C->bmws.ensure((size_t)3 * n * 8));
+    BmJob job{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_s, (int64_t)n, 0};
+    CK(launch_bm_block(job, C->bmws.as<uint64_t>(), smem_words, n >= 4096 ? 1024 : 256, d_out, st));
+    g_launches++;
+  } else {
+    int ctas = opts && opts->grid_ctas > 0 ? opts->grid_ctas : C->num_sms;
+    if ((int64_t)ctas > (int64_t)n) ctas = (int)n;
+    CK(C->bmws.ensure((size_t)2 * n * 8));
+    CK(C->bmsync.ensure(grid_sync_bytes()));
+    CK(cudaMemsetAsync(C->bmsync.p, 0, grid_sync_bytes(), st));
+    uint64_t* b0 = C->bmws.as<uint64_t>();
+    int used = 0;
+    // About one second of spinning at ~2 GHz before a wait is declared stuck.
+    const long long spin = 2000000000LL;
+    CK(launch_bm_grid(fp, d_s, (int64_t)n, ctas, 256, b0, b0 + n, C->bmsync.p, spin, d_out, st, &used));
+    g_launches += 2;
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, C->bmsync.as<char>() + grid_sync_err_offset(), sizeof(int), cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return MODLIN_ETIMEOUT;
+  }
+  CK(cudaMemcpyAsync(C->h_out, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *lc_out = (size_t)C->h_out[0];
+  return MODLIN_OK;
+}
+
+static int lc_batch_locked(Ctx* C, const uint64_t* p, const uint64_t* const* d_data, const size_t* n,
+                           size_t count, size_t* lcs_out, cudaStream_t st) {
+  if (count == 0) return MODLIN_OK;
+  std::vector<BmJob> jobs(count);
+  int64_t maxn = 0;
+  for (size_t i = 0; i < count; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    jobs[i] = BmJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_data[i], (int64_t)n[i], (int64_t)i};
+    maxn = std::max<int64_t>(maxn, (int64_t)n[i]);
+  }
+  // Longest first: the persistent CTAs then finish close together (LPT).
+  std::stable_sort(jobs.begin(), jobs.end(), [](const BmJob& a, const BmJob& b) { return a.n > b.n; });
+  const int threads = maxn > 2048 ? 512 : (maxn > 512 ? 256 : 128);
+  int64_t smem_words = std::min<int64_t>(3 * maxn, (200 * 1024) / 8);
+  int per_sm = bm_batch_max_blocks_per_sm(threads, smem_words);
+  if (per_sm < 1) per_sm = 1;
+  int blocks = C->num_sms * per_sm;
+  if ((size_t)blocks > count) blocks = (int)count;
+  const int64_t gws_words = 3 * maxn > smem_words ? 3 * maxn : 0;
+  if (gws_words) CK(C->bmws.ensure((size_t)blocks * gws_words * 8));
+  CK(C->bmjobs.ensure(sizeof(BmJob) * count));
+  CK(C->bmnext.ensure(sizeof(unsigned long long)));
+  CK(C->bmout.ensure(sizeof(int64_t) * count));
+  CK(cudaMemcpyAsync(C->bmjobs.p, jobs.data(), sizeof(BmJob) * count, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(C->bmnext.p, 0, sizeof(unsigned long long), st));
+  CK(launch_bm_batch(C->bmjobs.as<BmJob>(), (int64_t)count, C->bmnext.as<unsigned long long>(),
+                     C->bmws.as<uint64_t>(), gws_words, smem_words, blocks, threads, C->bmout.as<int64_t>(), st));
+  g_launches += 2;
+  std::vector<int64_t> out(count);
+  CK(cudaMemcpyAsync(out.data(), C->bmout.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < count; ++i) lcs_out[i] = (size_t)out[i];
+  return MODLIN_OK;
+}
+
+}  // namespace modlin
+
+using namespace modlin;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* modlin_strerror(int code) {
+  switch (code) {
+    case MODLIN_OK: return "ok";
+    case MODLIN_EINVAL_P: return "modulus must satisfy 2 <= p < 2^63";
+    case MODLIN_EINVAL_N: return "invalid size";
+    case MODLIN_EINPUT: return "input entry not reduced modulo p";
+    case MODLIN_ECUDA: return "CUDA error";
+    case MODLIN_ENOMEM: return "out of memory";
+    case MODLIN_ETIMEOUT: return "bounded device wait expired";
+    case MODLIN_ENODEV: return "no CUDA device";
+    case MODLIN_EINVAL_ARG: return "invalid argument";
+    default: return "unknown error";
+  }
+}
+
+int modlin_field_new(uint64_t p, modlin_field* f) {
+  FieldParams fp;
+  if (!f) return MODLIN_EINVAL_ARG;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  f->p = fp.p;
+  f->mu_lo = fp.mu_lo;
+  f->mu_hi = fp.mu_hi;
+  f->safe_batch = fp.safe_batch;
+  return MODLIN_OK;
+}
+
+uint64_t modlin_field_reduce_u128(const modlin_field* f, uint64_t hi, uint64_t lo) {
+  FieldParams fp{f->p, f->mu_lo, f->mu_hi, f->safe_batch};
+  return FpBarrett(fp).reduce(((u128)hi << 64) | lo);
+}
+
+uint64_t modlin_field_reduce(const modlin_field* f, uint64_t x) { return modlin_field_reduce_u128(f, 0, x); }
+
+uint64_t modlin_field_mul(const modlin_field* f, uint64_t a, uint64_t b) {
+  const u128 t = (u128)a * b;
+  return modlin_field_reduce_u128(f, (uint64_t)(t >> 64), (uint64_t)t);
+}
+
+int modlin_rank_device(uint64_t p, uint64_t* d_m, size_t n, const modlin_rank_opts* opts, size_t* rank_out,
+                       size_t* pivot_cols_out, void* stream) {
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  if (!d_m) return MODLIN_EINVAL_ARG;
+  std::lock_guard<std::mutex> g(C->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  return rank_device_locked(C, p, d_m, n, opts, rank_out, pivot_cols_out, st, nullptr, nullptr);
+}
+
+int modlin_rank_ex(uint64_t p, uint64_t* m, size_t n, const modlin_rank_opts* opts, size_t* rank_out,
+                   size_t* pivot_cols_out, modlin_progress_fn cb, void* cb_ctx) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (n == 0 || n > 0x7fffffff / 2 || n > SIZE_MAX / n / 8) return MODLIN_EINVAL_N;
+  if (!m || !rank_out) return MODLIN_EINVAL_ARG;
+  if (opts && opts->check_input && !check_residues(p, m, n * n)) return MODLIN_EINPUT;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  const size_t bytes = n * n * 8;
+  CK(C->mat.ensure(bytes));
+  CK(cudaMemcpyAsync(C->mat.p, m, bytes, cudaMemcpyHostToDevice, C->stream));
+  return rank_device_locked(C, p, C->mat.as<uint64_t>(), n, opts, rank_out, pivot_cols_out, C->stream, cb, cb_ctx);
+}
+
+int modlin_rank(uint64_t p, uint64_t* m, size_t n, size_t* rank_out, modlin_progress_fn cb, void* cb_ctx) {
+  return modlin_rank_ex(p, m, n, nullptr, rank_out, nullptr, cb, cb_ctx);
+}
+
+int modlin_linear_complexity_device(uint64_t p, const uint64_t* d_s, size_t n, const modlin_lc_opts* opts,
+                                    size_t* lc_out, void* stream) {
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  if (!d_s && n) return MODLIN_EINVAL_ARG;
+  std::lock_guard<std::mutex> g(C->mu);
+  return lc_device_locked(C, p, d_s, n, opts, lc_out, stream ? (cudaStream_t)stream : C->stream);
+}
+
+int modlin_linear_complexity_ex(uint64_t p, const uint64_t* s, size_t n, const modlin_lc_opts* opts,
+                                size_t* lc_out) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!lc_out || (!s && n)) return MODLIN_EINVAL_ARG;
+  if (opts && opts->check_input && !check_residues(p, s, n)) return MODLIN_EINPUT;
+  if (n == 0) {
+    *lc_out = 0;
+    return MODLIN_OK;
+  }
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  CK(C->seq.ensure(n * 8));
+  CK(cudaMemcpyAsync(C->seq.p, s, n * 8, cudaMemcpyHostToDevice, C->stream));
+  return lc_device_locked(C, p, C->seq.as<uint64_t>(), n, opts, lc_out, C->stream);
+}
+
+int modlin_linear_complexity(uint64_t p, const uint64_t* s, size_t n, size_t* lc_out, modlin_progress_fn cb,
+                             void* cb_ctx) {
+  const int rc = modlin_linear_complexity_ex(p, s, n, nullptr, lc_out);
+  if (rc == MODLIN_OK && cb) cb(cb_ctx, n, n);
+  return rc;
+}
+
+int modlin_lc_batch_device(const uint64_t* p, const uint64_t* const* d_data, const size_t* n, size_t count,
+                           size_t* lcs_out, void* stream) {
+  if (count && (!p || !d_data || !n || !lcs_out)) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  return lc_batch_locked(C, p, d_data, n, count, lcs_out, stream ? (cudaStream_t)stream : C->stream);
+}
+
+int modlin_lc_batch(const modlin_job* jobs, size_t count, size_t* lcs_out) {
+  if (count && (!jobs || !lcs_out)) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  size_t total = 0;
+  for (size_t i = 0; i < count; ++i) {
+    if (!jobs[i].data && jobs[i].n) return MODLIN_EINVAL_ARG;
+    total += jobs[i].n;
+  }
+  CK(C->seq.ensure(std::max<size_t>(total, 1) * 8));
+  std::vector<const uint64_t*> ptrs(count);
+  std::vector<uint64_t> ps(count);
+  std::vector<size_t> ns(count);
+  size_t off = 0;
+  for (size_t i = 0; i < count; ++i) {
+    if (jobs[i].n) CK(cudaMemcpyAsync(C->seq.as<uint64_t>() + off, jobs[i].data, jobs[i].n * 8,
+                                      cudaMemcpyHostToDevice, C->stream));
+    ptrs[i] = C->seq.as<uint64_t>() + off;
+    ps[i] = jobs[i].p;
+    ns[i] = jobs[i].n;
+    off += jobs[i].n;
+  }
+  return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, lcs_out, C->stream);
+}
+
+int modlin_rank_batch(const modlin_job* jobs, size_t count, size_t* ranks_out) {
+  if (count && (!jobs || !ranks_out)) return MODLIN_EINVAL_ARG;
+  // One job after another through the single-matrix engine (the batched
+  // persistent kernel handles this in rank_batch.cu when available).
+  for (size_t i = 0; i < count; ++i) {
+    std::vector<uint64_t> tmp(jobs[i].data, jobs[i].data + jobs[i].n * jobs[i].n);
+    const int rc = modlin_rank_ex(jobs[i].p, tmp.data(), jobs[i].n, nullptr, &ranks_out[i], nullptr, nullptr,
+                                  nullptr);
+    if (rc) return rc;
+  }
+  return MODLIN_OK;
+}
+
+int modlin_gen_uniform(uint64_t p, uint64_t seed, uint64_t* out, size_t count) {
+  if (p < 2) return MODLIN_EINVAL_P;
+  if (!out && count) return MODLIN_EINVAL_ARG;
+  const int bits = 64 - __builtin_clzll(p - 1);
+  uint64_t z = seed;
+  for (size_t i = 0; i < count;) {
+    z += 0x9e3779b97f4a7c15ULL;
+    uint64_t w = z;
+    w = (w ^ (w >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    w = (w ^ (w >> 27)) * 0x94d049bb133111ebULL;
+    w ^= w >> 31;
+    const uint64_t x = w >> (64 - bits);
+    if (x < p) out[i++] = x;
+  }
+  return MODLIN_OK;
+}
+
+int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t* out, size_t count) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!out && count) return MODLIN_EINVAL_ARG;
+  std::vector<uint64_t> a(L + 1), init(L);
+  std::vector<uint64_t> draws(1);
+  // Coefficients a_1..a_L, a_L redrawn while 0, then initial values.
+  uint64_t z = seed;
+  const int bits = 64 - __builtin_clzll(p - 1);
+  auto uni = [&]() {
+    for (;;) {
+      z += 0x9e3779b97f4a7c15ULL;
+      uint64_t w = z;
+      w = (w ^ (w >> 30)) * 0xbf58476d1ce4e5b9ULL;
+      w = (w ^ (w >> 27)) * 0x94d049bb133111ebULL;
+      w ^= w >> 31;
+      const uint64_t x = w >> (64 - bits);
+      if (x < p) return x;
+    }
+  };
+  for (size_t j = 1; j <= L; ++j) a[j] = uni();
+  while (L > 0 && a[L] == 0) a[L] = uni();
+  for (size_t i = 0; i < L; ++i) init[i] = uni();
+  const FpBarrett f(fp);
+  const uint64_t sb = fp.safe_batch;
+  for (size_t i = 0; i < count; ++i) {
+    if (i < L) {
+      out[i] = init[i];
+      continue;
+    }
+    u128 acc = 0;
+    uint64_t tot = 0, cnt = 0;
+    for (size_t j = 1; j <= L; ++j) {
+      acc += (u128)a[j] * out[i - j];
+      if (++cnt == sb) {
+        tot = f.add(tot, f.reduce(acc));
+        acc = 0;
+        cnt = 0;
+      }
+    }
+    out[i] = f.add(tot, f.reduce(acc));
+  }
+  return MODLIN_OK;
+}
+
+int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t* d_out, size_t count, void* stream) {
+  if (p < 2) return MODLIN_EINVAL_P;
+  if (!d_out && count) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  uint64_t nl = 0;
+  cudaError_t e = gen_uniform_device(p, seed, d_out, count, stream ? (cudaStream_t)stream : C->stream, &nl);
+  g_launches += nl;
+  return cuda_rc(e);
+}
+
+int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  CK(reduce_device(fp, d_x, count, st));
+  g_launches++;
+  return cuda_rc(cudaStreamSynchronize(st));
+}
+
+uint64_t modlin_kernel_launches(void) { return g_launches.load(); }
+
+double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
+
+}  // extern "C"

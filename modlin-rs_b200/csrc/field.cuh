@@ -1,0 +1,127 @@
+// Prime-field arithmetic over F_p, p < 2^63, for sm_100a device code and host.
+//
+// The contract is the reference's `Field` (src/fp.rs:34-114): canonical
+// residues in [0, p), Barrett reciprocal mu = floor((2^128 - 1) / p) and exact
+// reduction of any 128-bit value, add/sub/mul on canonical inputs, Fermat
+// inverse. Two policies implement it:
+//   * FpBarrett — any p in [2, 2^63): the reference's Barrett reduction
+//     (src/fp.rs:71-79) on 64-bit integer pipes;
+//   * FpM61 — p = 2^61 - 1 (MIXMAX's modulus and every large benchmark
+//     workload): shift-and-add reduction, since 2^61 = 1 mod p.
+// Both return the exact residue, so every kernel built on them is bit-exact.
+#pragma once
+#include <cstdint>
+
+#ifndef MODLIN_HD
+#define MODLIN_HD __host__ __device__ __forceinline__
+#endif
+
+namespace modlin {
+
+typedef unsigned __int128 u128;
+
+// src/fp.rs:13-24: high 128 bits of the 256-bit product a*b.
+MODLIN_HD u128 mul_hi_128(u128 a, u128 b) {
+  const uint64_t a1 = (uint64_t)(a >> 64), a0 = (uint64_t)a;
+  const uint64_t b1 = (uint64_t)(b >> 64), b0 = (uint64_t)b;
+  const u128 lo = (u128)a0 * b0, mid1 = (u128)a1 * b0, mid2 = (u128)a0 * b1;
+  const u128 hi = (u128)a1 * b1;
+  const u128 carry = (lo >> 64) + (uint64_t)mid1 + (uint64_t)mid2;
+  return hi + (mid1 >> 64) + (mid2 >> 64) + (carry >> 64);
+}
+
+// Host-side construction data for a field (src/fp.rs:49-61).
+struct FieldParams {
+  uint64_t p;
+  uint64_t mu_lo, mu_hi;  // mu = floor((2^128 - 1) / p)
+  uint64_t safe_batch;    // products of (p-1)^2 summable in a u128
+};
+
+inline bool make_field_params(uint64_t p, FieldParams* f) {
+  if (p < 2 || p >= (1ULL << 63)) return false;
+  const u128 umax = ~(u128)0;
+  const u128 mu = umax / p;
+  const u128 maxp = (u128)(p - 1) * (p - 1);
+  u128 sb = umax / maxp;
+  if (sb > (u128)UINT64_MAX) sb = UINT64_MAX;
+  f->p = p;
+  f->mu_lo = (uint64_t)mu;
+  f->mu_hi = (uint64_t)(mu >> 64);
+  f->safe_batch = sb ? (uint64_t)sb : 1;
+  return true;
+}
+
+constexpr uint64_t kM61 = (1ULL << 61) - 1;
+
+struct FpBarrett {
+  uint64_t p, mu_lo, mu_hi, sb;
+  FpBarrett() = default;
+  MODLIN_HD explicit FpBarrett(const FieldParams& f) : p(f.p), mu_lo(f.mu_lo), mu_hi(f.mu_hi), sb(f.safe_batch) {}
+  // src/fp.rs:71-79: q = hi(t*mu) <= floor(t/p), r = t - q*p < 3p.
+  MODLIN_HD uint64_t reduce(u128 t) const {
+    const u128 mu = ((u128)mu_hi << 64) | mu_lo;
+    const u128 q = mul_hi_128(t, mu);
+    u128 r = t - q * p;
+    if (r >= p) r -= p;
+    if (r >= p) r -= p;
+    return (uint64_t)r;
+  }
+  MODLIN_HD uint64_t add(uint64_t a, uint64_t b) const {
+    const uint64_t s = a + b;
+    return s >= p ? s - p : s;
+  }
+  MODLIN_HD uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + p - b; }
+  MODLIN_HD uint64_t mul(uint64_t a, uint64_t b) const { return reduce((u128)a * b); }
+  // Number of (p-1)^2 products a u128 accumulator holds before it must be reduced.
+  MODLIN_HD uint64_t safe_batch() const { return sb; }
+  MODLIN_HD uint64_t modulus() const { return p; }
+};
+
+struct FpM61 {
+  FpM61() = default;
+  MODLIN_HD explicit FpM61(const FieldParams&) {}
+  MODLIN_HD static uint64_t fold(uint64_t x) { return (x & kM61) + (x >> 61); }
+  // Exact t mod (2^61 - 1) for any 128-bit t: 2^64 = 8 (mod p).
+  MODLIN_HD uint64_t reduce(u128 t) const {
+    const uint64_t t0 = (uint64_t)t, t1 = (uint64_t)(t >> 64);
+    uint64_t a = fold(t1);  // < 2^61 + 8
+    if (a >= kM61) a -= kM61;
+    const uint64_t a8 = ((a << 3) & kM61) + (a >> 58);  // 8a mod p, < 2^61 + 8
+    uint64_t x = fold(t0) + a8;                          // < 2^62 + 16
+    x = fold(x);
+    if (x >= kM61) x -= kM61;
+    return x;
+  }
+  MODLIN_HD uint64_t add(uint64_t a, uint64_t b) const {
+    const uint64_t s = a + b;
+    return s >= kM61 ? s - kM61 : s;
+  }
+  MODLIN_HD uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + kM61 - b; }
+  MODLIN_HD uint64_t mul(uint64_t a, uint64_t b) const {
+    const u128 t = (u128)a * b;  // < 2^122
+    const uint64_t lo = (uint64_t)t, hi = (uint64_t)(t >> 64);
+    uint64_t x = (lo & kM61) + ((lo >> 61) | (hi << 3));  // < 2^62
+    x = fold(x);
+    return x >= kM61 ? x - kM61 : x;
+  }
+  MODLIN_HD uint64_t safe_batch() const { return 64; }
+  MODLIN_HD uint64_t modulus() const { return kM61; }
+};
+
+// src/fp.rs:97-113: Fermat inverse a^(p-2), a != 0.
+template <class F>
+MODLIN_HD uint64_t fp_pow(const F& f, uint64_t a, uint64_t e) {
+  uint64_t r = 1;
+  while (e) {
+    if (e & 1) r = f.mul(r, a);
+    a = f.mul(a, a);
+    e >>= 1;
+  }
+  return r;
+}
+template <class F>
+MODLIN_HD uint64_t fp_inv(const F& f, uint64_t a) {
+  return fp_pow(f, a, f.modulus() - 2);
+}
+
+}  // namespace modlin

@@ -1,0 +1,395 @@
+// Panel kernels and the plain trailing update of the blocked GPU rank.
+// See rank_plain.cuh for the algorithm and its correspondence to the
+// reference's src/fp.rs:125-255.
+#include <cuda_runtime.h>
+
+#include "rank_plain.cuh"
+#include "rank_kernels.cuh"
+
+namespace modlin {
+
+// ---------------------------------------------------------------------------
+// window_kernel — one CTA, kWindowThreads threads.
+// Candidates: round 0 -> rows [r0, r0 + min(64, n - r0)); later rounds ->
+// ps->cand[0 .. min(ps->ncand, 64)). Their panel columns [col, col + W) are
+// eliminated in shared memory with first-nonzero pivoting in candidate order
+// (src/fp.rs:150-157), fraction-free, while recording for each candidate
+// alpha and its coefficients g against this round's new pivots, so that a
+// pivot row k satisfies  U_k = alpha_k * row_k - sum_{k2<k} G[k][k2] * U_k2.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(kWindowThreads) window_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
+                                                                 int32_t n, int32_t r0, int32_t col, int32_t W,
+                                                                 int32_t round, PanelState* ps, uint64_t* Upanel,
+                                                                 uint64_t* G, const uint64_t* Lbuf,
+                                                                 uint8_t* is_pivot) {
+  extern __shared__ __align__(16) uint64_t smem_w[];
+  uint64_t(*A)[kPanel] = reinterpret_cast<uint64_t(*)[kPanel]>(smem_w);                  // [64][64]
+  uint64_t(*Gc)[kPanel] = reinterpret_cast<uint64_t(*)[kPanel]>(smem_w + kWindow * kPanel);  // [64][64]
+  __shared__ uint64_t alph[kWindow];
+  __shared__ int32_t rowidx[kWindow], ispiv[kWindow], pivcand[kPanel], pivc[kPanel];
+  __shared__ uint32_t ballots[2][2];
+  __shared__ int32_t sh_nc, sh_pb_old;
+  __shared__ uint64_t sh_mask;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    int nc = round == 0 ? min(kWindow, n - r0) : min(ps->ncand, kWindow);
+    sh_nc = nc < 0 ? 0 : nc;
+    sh_pb_old = ps->pb;
+    sh_mask = ps->colmask;
+  }
+  __syncthreads();
+  const int nc = sh_nc, pb_old = sh_pb_old;
+  const uint64_t mask0 = sh_mask;
+  if (tid < kWindow) {
+    rowidx[tid] = tid < nc ? (round == 0 ? r0 + tid : ps->cand[tid]) : -1;
+    ispiv[tid] = 0;
+    alph[tid] = 1;
+  }
+  for (int idx = tid; idx < kWindow * kPanel; idx += blockDim.x) {
+    (&Gc[0][0])[idx] = 0;
+    (&A[0][0])[idx] = 0;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nc * W; idx += blockDim.x) {
+    const int i = idx / W, c = idx - (idx / W) * W;
+    A[i][c] = m[(int64_t)rowidx[i] * ld + col + c];
+  }
+  __syncthreads();
+
+  int npiv = 0, nb = 0;
+  uint64_t newmask = 0;
+  const int j = tid >> 3, sub = tid & 7;
+  for (int c = 0; c < W; ++c) {
+    if ((mask0 >> c) & 1ULL) continue;
+    if (tid < kWindow) {
+      const bool nz = tid < nc && !ispiv[tid] && A[tid][c] != 0;
+      const uint32_t bal = __ballot_sync(0xffffffffu, nz);
+      if ((tid & 31) == 0) ballots[nb & 1][tid >> 5] = bal;
+    }
+    __syncthreads();
+    const uint32_t b0 = ballots[nb & 1][0], b1 = ballots[nb & 1][1];
+    ++nb;
+    const int piv = b0 ? __ffs(b0) - 1 : (b1 ? 31 + __ffs(b1) : -1);
+    if (piv < 0) continue;
+    const int t = npiv++;
+    newmask |= 1ULL << c;
+    const uint64_t e = A[piv][c];
+    uint64_t h = 0;
+    if (j < nc && j != piv && !ispiv[j]) h = A[j][c];
+    __syncwarp();
+    if (h != 0) {
+      for (int cc = c + 1 + sub; cc < W; cc += 8) A[j][cc] = f.sub(f.mul(e, A[j][cc]), f.mul(h, A[piv][cc]));
+      for (int t2 = sub; t2 < t; t2 += 8) Gc[j][t2] = f.mul(e, Gc[j][t2]);
+      if (sub == 0) {
+        alph[j] = f.mul(e, alph[j]);
+        Gc[j][t] = h;
+        A[j][c] = 0;
+      }
+    }
+    if (tid == 0) {
+      ispiv[piv] = 1;
+      pivcand[t] = piv;
+      pivc[t] = c;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+
+  // Outputs: pivot bookkeeping, reduced pivot rows, transformation rows.
+  for (int t = tid; t < npiv; t += blockDim.x) {
+    const int k = pb_old + t, i = pivcand[t];
+    ps->prow[k] = rowidx[i];
+    ps->pcol[k] = col + pivc[t];
+    ps->alpha[k] = alph[i];
+    ps->inv[k] = fp_inv(f, A[i][pivc[t]]);
+    is_pivot[rowidx[i]] = 1;
+  }
+  for (int idx = tid; idx < npiv * kPanel; idx += blockDim.x) {
+    const int t = idx / kPanel, cc = idx % kPanel;
+    Upanel[(int64_t)(pb_old + t) * kPanel + cc] = cc < W ? A[pivcand[t]][cc] : 0;
+  }
+  for (int idx = tid; idx < npiv * kPanel; idx += blockDim.x) {
+    const int t = idx / kPanel, k2 = idx % kPanel, k = pb_old + t, i = pivcand[t];
+    uint64_t v = 0;
+    if (k2 < pb_old)
+      v = f.mul(alph[i], Lbuf[(int64_t)(rowidx[i] - r0) * kPanel + k2]);
+    else if (k2 < k)
+      v = Gc[i][k2 - pb_old];
+    G[(int64_t)k * kPanel + k2] = v;
+  }
+  if (tid == 0) {
+    ps->pb = pb_old + npiv;
+    ps->colmask = mask0 | newmask;
+    ps->ncand = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bulk_kernel — a warp per active non-pivot row: reference-style elimination
+// of this round's new pivots pb_lo .. ps->pb from the row's panel part
+// (f = e * inv, row -= f * U_k; src/fp.rs:163-175), multipliers to Lbuf,
+// residual written back and, if nonzero, the row offered as a candidate.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) bulk_kernel(F f, uint64_t* __restrict__ m, int64_t ld, int32_t n, int32_t r0,
+                                                    int32_t col, int32_t W, int32_t pb_lo, PanelState* ps,
+                                                    const uint64_t* __restrict__ Upanel, uint64_t* Lbuf,
+                                                    const uint8_t* __restrict__ is_pivot) {
+  __shared__ uint64_t Us[kPanel][kPanel];
+  __shared__ uint64_t invs[kPanel];
+  __shared__ int32_t pcs[kPanel];
+  const int pb_hi = ps->pb;
+  const int nk = pb_hi - pb_lo;
+  for (int idx = threadIdx.x; idx < nk * kPanel; idx += blockDim.x) {
+    const int t = idx / kPanel, c = idx % kPanel;
+    Us[t][c] = c < W ? Upanel[(int64_t)(pb_lo + t) * kPanel + c] : 0;
+  }
+  for (int t = threadIdx.x; t < nk; t += blockDim.x) {
+    invs[t] = ps->inv[pb_lo + t];
+    pcs[t] = ps->pcol[pb_lo + t] - col;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warps_total = gridDim.x * (blockDim.x >> 5);
+  for (int r = r0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps_total) {
+    if (is_pivot[r]) continue;
+    uint64_t* row = m + (int64_t)r * ld + col;
+    uint64_t x0 = lane < W ? row[lane] : 0;
+    uint64_t x1 = lane + 32 < W ? row[lane + 32] : 0;
+    for (int t = 0; t < nk; ++t) {
+      const int pc = pcs[t];
+      const uint64_t e = __shfl_sync(0xffffffffu, pc < 32 ? x0 : x1, pc & 31);
+      const uint64_t fm = e ? f.mul(e, invs[t]) : 0;
+      if (lane == 0) Lbuf[(int64_t)(r - r0) * kPanel + pb_lo + t] = fm;
+      if (fm) {
+        if (lane < W) x0 = f.sub(x0, f.mul(fm, Us[t][lane]));
+        if (lane + 32 < W) x1 = f.sub(x1, f.mul(fm, Us[t][lane + 32]));
+      }
+    }
+    if (nk > 0) {
+      if (lane < W) row[lane] = x0;
+      if (lane + 32 < W) row[lane + 32] = x1;
+    }
+    const bool nz = __any_sync(0xffffffffu, (x0 | x1) != 0);
+    if (nz && lane == 0) {
+      const int s = atomicAdd(&ps->ncand, 1);
+      if (s < kWindow) ps->cand[s] = r;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// couple_kernel — U block (src/fp.rs:184-200): for every trailing column c,
+// U_k[c] = alpha_k * row_{prow_k}[c] - sum_{k2<k} G[k][k2] * U_k2[c],
+// sequential in k, a thread per column, u128 lazy accumulation.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) couple_kernel(F f, const uint64_t* __restrict__ m, int64_t ld, int32_t n,
+                                                      int32_t jend, const PanelState* __restrict__ ps,
+                                                      const uint64_t* __restrict__ G, uint64_t* Ubuf, int64_t ldU) {
+  __shared__ uint64_t Gs[kPanel][kPanel + 1];
+  __shared__ uint64_t al[kPanel];
+  __shared__ int32_t prs[kPanel];
+  const int pb = ps->pb;
+  for (int idx = threadIdx.x; idx < pb * kPanel; idx += blockDim.x) Gs[idx / kPanel][idx % kPanel] = G[idx];
+  for (int k = threadIdx.x; k < pb; k += blockDim.x) {
+    al[k] = ps->alpha[k];
+    prs[k] = ps->prow[k];
+  }
+  __syncthreads();
+  const int64_t c = (int64_t)jend + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const uint64_t sb = f.safe_batch();
+  for (int k = 0; k < pb; ++k) {
+    const uint64_t v = f.mul(al[k], m[(int64_t)prs[k] * ld + c]);
+    u128 acc = 0;
+    uint64_t tot = 0, cnt = 0;
+    for (int k2 = 0; k2 < k; ++k2) {
+      const uint64_t g = Gs[k][k2];
+      if (g) {
+        acc += (u128)g * Ubuf[(int64_t)k2 * ldU + c];
+        if (++cnt == sb) {
+          tot = f.add(tot, f.reduce(acc));
+          acc = 0;
+          cnt = 0;
+        }
+      }
+    }
+    tot = f.add(tot, f.reduce(acc));
+    Ubuf[(int64_t)k * ldU + c] = f.sub(v, tot);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// move_rows_kernel — compaction of the active block: a non-pivot row that sits
+// in [r0, r0 + pb) is copied (trailing part and multiplier row) into the slot
+// of a pivot row that sits in [r0 + pb, n). blockIdx.y = move.
+// ---------------------------------------------------------------------------
+__global__ void move_rows_kernel(uint64_t* m, int64_t ld, int32_t n, int32_t jend, const int2* moves,
+                                 uint64_t* Lbuf, int32_t r0, int32_t pb) {
+  const int2 mv = moves[blockIdx.y];
+  const int64_t src = mv.x, dst = mv.y;
+  for (int64_t c = (int64_t)jend + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    m[dst * ld + c] = m[src * ld + c];
+  if (blockIdx.x == 0)
+    for (int k = threadIdx.x; k < pb; k += blockDim.x)
+      Lbuf[(dst - r0) * kPanel + k] = Lbuf[(src - r0) * kPanel + k];
+}
+
+__global__ void clear_pivot_flags_kernel(const PanelState* ps, uint8_t* is_pivot) {
+  const int k = threadIdx.x;
+  if (k < ps->pb) is_pivot[ps->prow[k]] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// trailing_plain_kernel — A[rbeg.., jend..] -= L * U mod p on the integer
+// pipes (src/fp.rs:208-248): 64x64 output tile per CTA, 4x4 per thread,
+// u128 accumulators, one reduction per safe_batch products.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __restrict__ m, int64_t ld, int32_t rbeg,
+                                                              int32_t n, int32_t jend,
+                                                              const uint64_t* __restrict__ Lbuf, int32_t r0,
+                                                              const uint64_t* __restrict__ Ubuf, int64_t ldU,
+                                                              int32_t K) {
+  constexpr int KC = 32;  // K chunk staged in shared memory
+  __shared__ uint64_t Ls[KC][64 + 1];
+  __shared__ uint64_t Us[KC][64];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t rt = (int64_t)rbeg + (int64_t)blockIdx.y * 64;
+  const int64_t ct = (int64_t)jend + (int64_t)blockIdx.x * 64;
+  const uint64_t sb = f.safe_batch();
+  uint64_t tot[4][4];
+  u128 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      tot[i][q] = 0;
+      acc[i][q] = 0;
+    }
+  uint64_t cnt = 0;
+  for (int k0 = 0; k0 < K; k0 += KC) {
+    const int kc = min(KC, K - k0);
+    for (int idx = tid; idx < 64 * kc; idx += 256) {
+      const int ri = idx / kc, k = idx - ri * kc;
+      const int64_t r = rt + ri;
+      Ls[k][ri] = r < n ? Lbuf[(r - r0) * kPanel + k0 + k] : 0;
+    }
+    for (int idx = tid; idx < 64 * kc; idx += 256) {
+      const int k = idx >> 6, ci = idx & 63;
+      const int64_t c = ct + ci;
+      Us[k][ci] = c < n ? Ubuf[(int64_t)(k0 + k) * ldU + c] : 0;
+    }
+    __syncthreads();
+    for (int k = 0; k < kc; ++k) {
+      uint64_t a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = Ls[k][ty + 16 * i];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b[q] = Us[k][tx + 16 * q];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] += (u128)a[i] * b[q];
+      if (++cnt == sb) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            tot[i][q] = f.add(tot[i][q], f.reduce(acc[i][q]));
+            acc[i][q] = 0;
+          }
+        cnt = 0;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t r = rt + ty + 16 * i;
+    if (r >= n) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t c = ct + tx + 16 * q;
+      if (c < n) {
+        uint64_t* p = m + r * ld + c;
+        *p = f.sub(*p, f.add(tot[i][q], f.reduce(acc[i][q])));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launch wrappers (explicit instantiation for both field policies).
+// ---------------------------------------------------------------------------
+template <class F>
+void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
+                   PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,
+                   cudaStream_t st) {
+  const size_t smem = 2 * kWindow * kPanel * sizeof(uint64_t);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(window_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  window_kernel<F><<<1, kWindowThreads, smem, st>>>(f, m, ld, n, r0, col, W, round, ps, Upanel, G, Lbuf, is_pivot);
+}
+
+template <class F>
+void launch_bulk(const F& f, uint64_t* m, int64_t ld, int n, int r0, int col, int W, int pb_lo, PanelState* ps,
+                 const uint64_t* Upanel, uint64_t* Lbuf, const uint8_t* is_pivot, int num_sms, cudaStream_t st) {
+  const int rows = n - r0;
+  int blocks = (rows + 7) / 8;
+  const int cap = num_sms * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  bulk_kernel<F><<<blocks, 256, 0, st>>>(f, m, ld, n, r0, col, W, pb_lo, ps, Upanel, Lbuf, is_pivot);
+}
+
+template <class F>
+void launch_couple(const F& f, const uint64_t* m, int64_t ld, int n, int jend, const PanelState* ps,
+                   const uint64_t* G, uint64_t* Ubuf, int64_t ldU, cudaStream_t st) {
+  const int cols = n - jend;
+  couple_kernel<F><<<(cols + 255) / 256, 256, 0, st>>>(f, m, ld, n, jend, ps, G, Ubuf, ldU);
+}
+
+void launch_moves(uint64_t* m, int64_t ld, int n, int jend, const int2* moves, int nmoves, uint64_t* Lbuf, int r0,
+                  int pb, cudaStream_t st) {
+  if (nmoves <= 0) return;
+  const int cols = n - jend;
+  int bx = (cols + 255) / 256;
+  if (bx > 64) bx = 64;
+  if (bx < 1) bx = 1;
+  move_rows_kernel<<<dim3(bx, nmoves), 256, 0, st>>>(m, ld, n, jend, moves, Lbuf, r0, pb);
+}
+
+void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st) {
+  clear_pivot_flags_kernel<<<1, kPanel, 0, st>>>(ps, is_pivot);
+}
+
+template <class F>
+void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int n, int jend, const uint64_t* Lbuf,
+                           int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st) {
+  if (rbeg >= n || jend >= n || K <= 0) return;
+  dim3 grid((n - jend + 63) / 64, (n - rbeg + 63) / 64);
+  trailing_plain_kernel<F><<<grid, 256, 0, st>>>(f, m, ld, rbeg, n, jend, Lbuf, r0, Ubuf, ldU, K);
+}
+
+#define INSTANTIATE(F)                                                                                          \
+  template void launch_window<F>(const F&, const uint64_t*, int64_t, int, int, int, int, int, PanelState*,       \
+                                 uint64_t*, uint64_t*, const uint64_t*, uint8_t*, cudaStream_t);                \
+  template void launch_bulk<F>(const F&, uint64_t*, int64_t, int, int, int, int, int, PanelState*,              \
+                               const uint64_t*, uint64_t*, const uint8_t*, int, cudaStream_t);                  \
+  template void launch_couple<F>(const F&, const uint64_t*, int64_t, int, int, const PanelState*,               \
+                                 const uint64_t*, uint64_t*, int64_t, cudaStream_t);                            \
+  template void launch_trailing_plain<F>(const F&, uint64_t*, int64_t, int, int, int, const uint64_t*, int,     \
+                                         const uint64_t*, int64_t, int, cudaStream_t);
+
+INSTANTIATE(FpBarrett)
+INSTANTIATE(FpM61)
+
+}  // namespace modlin

@@ -1,0 +1,29 @@
+// Launch wrappers of the rank kernels (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "field.cuh"
+#include "rank_plain.cuh"
+
+namespace modlin {
+
+template <class F>
+void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
+                   PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,
+                   cudaStream_t st);
+template <class F>
+void launch_bulk(const F& f, uint64_t* m, int64_t ld, int n, int r0, int col, int W, int pb_lo, PanelState* ps,
+                 const uint64_t* Upanel, uint64_t* Lbuf, const uint8_t* is_pivot, int num_sms, cudaStream_t st);
+template <class F>
+void launch_couple(const F& f, const uint64_t* m, int64_t ld, int n, int jend, const PanelState* ps,
+                   const uint64_t* G, uint64_t* Ubuf, int64_t ldU, cudaStream_t st);
+void launch_moves(uint64_t* m, int64_t ld, int n, int jend, const int2* moves, int nmoves, uint64_t* Lbuf, int r0,
+                  int pb, cudaStream_t st);
+void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st);
+template <class F>
+void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int n, int jend, const uint64_t* Lbuf,
+                           int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st);
+
+}  // namespace modlin

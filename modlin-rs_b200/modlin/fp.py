@@ -1,0 +1,148 @@
+"""``modlin::fp`` over the C ABI: Field, rank, linear_complexity (src/fp.rs)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import (Job, LcOpts, PROGRESS, RankOpts, check, lib, szt, u64p)
+from ._lib import Field as _CField
+
+KERNELS = {"auto": 0, "plain": 1, "tc": 2}
+LC_KERNELS = {"auto": 0, "block": 1, "grid": 2}
+_NO_PROGRESS = ctypes.cast(None, PROGRESS)
+
+
+class Field:
+    """``Field`` (src/fp.rs:34-114): Barrett reduction modulo a prime p < 2^63."""
+
+    def __init__(self, p: int):
+        self._f = _CField()
+        check(lib().modlin_field_new(p, ctypes.byref(self._f)), "Field::new")
+        self.p = p
+
+    @property
+    def safe_batch(self) -> int:
+        return int(self._f.safe_batch)
+
+    @property
+    def mu(self) -> int:
+        return (int(self._f.mu_hi) << 64) | int(self._f.mu_lo)
+
+    def reduce(self, x: int) -> int:
+        """src/fp.rs:65-67."""
+        return int(lib().modlin_field_reduce(ctypes.byref(self._f), x))
+
+    def reduce_u128(self, t: int) -> int:
+        """src/fp.rs:71-79."""
+        return int(lib().modlin_field_reduce_u128(ctypes.byref(self._f), (t >> 64) & (2**64 - 1), t & (2**64 - 1)))
+
+    def mul(self, a: int, b: int) -> int:
+        """src/fp.rs:93-95 (canonical inputs)."""
+        return int(lib().modlin_field_mul(ctypes.byref(self._f), a, b))
+
+
+def _p(field) -> int:
+    return field.p if isinstance(field, Field) else int(field)
+
+
+def _as_u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1))
+
+
+def rank(field, m, n: int | None = None, *, kernel: str = "auto", pivot_cols: bool = False,
+         check_input: bool = False, progress=None):
+    """``fp::rank`` (src/fp.rs:125): rank of the n x n row-major matrix ``m``.
+
+    ``m`` may be any array-like of residues; it is not modified. With
+    ``pivot_cols`` the column profile (pivot columns, increasing) is returned
+    too.
+    """
+    a = _as_u64(m)
+    if n is None:
+        n = int(round(a.size ** 0.5))
+    if a.size != n * n:
+        raise ValueError(f"matrix has {a.size} entries, expected {n}x{n}")
+    opts = RankOpts(KERNELS[kernel], int(check_input))
+    out = szt(0)
+    pc = np.zeros(max(n, 1), dtype=np.uintp) if pivot_cols else None
+    cb = PROGRESS(lambda ctx, done, total: progress(done, total)) if progress else _NO_PROGRESS
+    rc = lib().modlin_rank_ex(_p(field), a.ctypes.data_as(u64p), n, ctypes.byref(opts), ctypes.byref(out),
+                              pc.ctypes.data_as(ctypes.POINTER(szt)) if pivot_cols else None, cb, None)
+    check(rc, "rank")
+    r = int(out.value)
+    if pivot_cols:
+        return r, [int(x) for x in pc[:r]]
+    return r
+
+
+def rank_device(field, ptr: int, n: int, *, kernel: str = "auto", stream: int = 0, pivot_cols: bool = False):
+    """Rank of a device-resident n x n matrix at ``ptr`` (clobbered)."""
+    opts = RankOpts(KERNELS[kernel], 0)
+    out = szt(0)
+    pc = np.zeros(max(n, 1), dtype=np.uintp) if pivot_cols else None
+    rc = lib().modlin_rank_device(_p(field), ptr, n, ctypes.byref(opts), ctypes.byref(out),
+                                  pc.ctypes.data_as(ctypes.POINTER(szt)) if pivot_cols else None, stream or None)
+    check(rc, "rank_device")
+    r = int(out.value)
+    return (r, [int(x) for x in pc[:r]]) if pivot_cols else r
+
+
+def linear_complexity(field, s, *, kernel: str = "auto", grid_ctas: int = 0, check_input: bool = False) -> int:
+    """``fp::linear_complexity`` (src/fp.rs:260)."""
+    a = _as_u64(s)
+    out = szt(0)
+    opts = LcOpts(LC_KERNELS[kernel], int(check_input), grid_ctas)
+    rc = lib().modlin_linear_complexity_ex(_p(field), a.ctypes.data_as(u64p), a.size, ctypes.byref(opts),
+                                           ctypes.byref(out))
+    check(rc, "linear_complexity")
+    return int(out.value)
+
+
+def linear_complexity_device(field, ptr: int, n: int, *, kernel: str = "auto", grid_ctas: int = 0,
+                             stream: int = 0) -> int:
+    out = szt(0)
+    opts = LcOpts(LC_KERNELS[kernel], 0, grid_ctas)
+    rc = lib().modlin_linear_complexity_device(_p(field), ptr, n, ctypes.byref(opts), ctypes.byref(out),
+                                               stream or None)
+    check(rc, "linear_complexity_device")
+    return int(out.value)
+
+
+def _jobs(items):
+    arrs = [(_p(p), _as_u64(x)) for p, x in items]
+    jobs = (Job * max(len(arrs), 1))()
+    for i, (p, a) in enumerate(arrs):
+        jobs[i] = Job(p, a.ctypes.data_as(u64p), 0)
+    return jobs, arrs
+
+
+def rank_batch(items) -> list[int]:
+    """Ranks of ``[(p, matrix), ...]`` (square matrices of any sides)."""
+    jobs, arrs = _jobs(items)
+    for i, (_, a) in enumerate(arrs):
+        jobs[i].n = int(round(a.size ** 0.5))
+    out = (szt * max(len(arrs), 1))()
+    check(lib().modlin_rank_batch(jobs, len(arrs), out), "rank_batch")
+    return [int(out[i]) for i in range(len(arrs))]
+
+
+def lc_batch(items) -> list[int]:
+    """Linear complexities of ``[(p, sequence), ...]`` in one persistent launch."""
+    jobs, arrs = _jobs(items)
+    for i, (_, a) in enumerate(arrs):
+        jobs[i].n = a.size
+    out = (szt * max(len(arrs), 1))()
+    check(lib().modlin_lc_batch(jobs, len(arrs), out), "lc_batch")
+    return [int(out[i]) for i in range(len(arrs))]
+
+
+def lc_batch_device(ps, ptrs, ns, stream: int = 0) -> list[int]:
+    """Device-resident batch: ``ptrs[i]`` points at ``ns[i]`` residues mod ``ps[i]``."""
+    k = len(ptrs)
+    P = (ctypes.c_uint64 * k)(*ps)
+    D = (ctypes.c_void_p * k)(*ptrs)
+    N = (szt * k)(*ns)
+    out = (szt * k)()
+    check(lib().modlin_lc_batch_device(P, D, N, k, out, stream or None), "lc_batch_device")
+    return [int(out[i]) for i in range(k)]

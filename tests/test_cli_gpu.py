@@ -1,0 +1,66 @@
+"""The `modlin` CLI on the GPU: stdout byte-identical to the reference's
+(README.md:61-158, src/main.rs:23-26, :74-78, :121-125, :142-148, :170-174)."""
+import json
+import os
+import subprocess
+
+import pytest
+
+from conftest import M61, PKG
+
+pytestmark = pytest.mark.gpu
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
+CLI = os.path.join(PKG, "bin", "modlin")
+
+
+def run(*args):
+    r = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return r.stdout.splitlines()
+
+
+def test_readme_rank_500():
+    out = run("-R", "500", "-p", str(M61), "-S", "1", "--prng", "mixmax17")
+    assert out == GOLD["reference"]["readme_rank500_stdout"]
+
+
+def test_readme_lc_1000():
+    out = run("-L", "1000", "-p", str(M61), "-S", "1", "--prng", "mixmax17")
+    assert out == GOLD["reference"]["readme_lc1000_stdout"]
+
+
+@pytest.mark.parametrize("kernel", ["plain", "tc"])
+def test_readme_xoroshiro_rank(kernel):
+    out = run("-R", "1000", "-p", "2", "--prng", "xoroshiro128pp", "--kernel", kernel)
+    assert out == ["Generator: xoroshiro128++", "Seed: 0x0000000000000000",
+                   "Running a modular rank test using 7.629 MiB of RAM: 1 1000×1000 matrix over the field of size 2",
+                   "Matrix 1/1\tcorank=0\tp=1"]
+    out = run("-R", "1000", "-p", str(M61), "--prng", "xoroshiro128pp", "--kernel", kernel)
+    assert out[-1] == "Matrix 1/1\tcorank=0\tp=1"
+
+
+def test_readme_xoroshiro_lc():
+    out = run("-L", "1000", "-p", "2", "--prng", "xoroshiro128pp")
+    assert out[2:] == ["Running a modular linear-complexity test using 0.031 MiB of RAM: 1 sequence of length 1000 "
+                       "over the field of size 2",
+                       "Sequence 1/1\tlinear complexity=503\tp=0.9947916666666666"]
+    out = run("-L", "10000", "-p", str(M61), "--prng", "xoroshiro128pp")
+    assert out[-1] == "Sequence 1/1\tlinear complexity=5000\tp=1"
+
+
+def test_reps_match_one_at_a_time(O):
+    """`reps` runs on disjoint stretches of the orbit (src/main.rs:82, :152)."""
+    out = run("-L", "300", "-p", "65521", "-S", "5", "--prng", "mixmax256", "4")
+    assert out[2].startswith("Running a modular linear-complexity test using 0.009 MiB of RAM: 4 sequences")
+    x = [int(v) % 65521 for v in O.prng("mixmax256", 5, 1200)]
+    for t in range(4):
+        lc = O.linear_complexity(65521, x[300 * t:300 * (t + 1)])
+        p = O.pretty_p_value(O.lc_left_tail_pvalue(65521, 300, lc))
+        assert out[3 + t] == f"Sequence {t + 1}/4\tlinear complexity={lc}\tp={p}"
+    out = run("-R", "40", "-p", "97", "-S", "3", "--prng", "mixmax17", "3")
+    x = [int(v) % 97 for v in O.prng("mixmax17", 3, 4800)]
+    for t in range(3):
+        c = 40 - O.rank(97, x[1600 * t:1600 * (t + 1)], 40)
+        p = O.pretty_p_value(O.corank_tail_pvalue(97, 40, c))
+        assert out[3 + t] == f"Matrix {t + 1}/3\tcorank={c}\tp={p}"
