@@ -250,7 +250,7 @@ def main():
     kernel = args.kernel
     if kernel == "auto":
         try:
-            modlin.rank(M61, np.eye(2, dtype=np.uint64), 2, kernel="tc")
+            modlin.rank(M61, np.eye(130, dtype=np.uint64), 130, kernel="tc")
             kernel = "tc"
         except modlin.ModlinError:
             kernel = "plain"

@@ -53,6 +53,7 @@ struct Ctx {
   // rank workspaces
   DevBuf mat, lbuf, ubuf, upanel, gmat, pstate, ispiv, moves;
   DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
+  DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
   PanelState* h_ps = nullptr;
   int2* h_moves = nullptr;
   // linear-complexity workspaces
@@ -65,6 +66,9 @@ static std::mutex g_ctx_mu;
 static Ctx* g_ctx[64];
 
 static int get_ctx(Ctx** out) {
+  // A failed earlier call may have left a (non-sticky) error in the runtime's
+  // last-error slot; it must not be reported by this call.
+  cudaGetLastError();
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return MODLIN_ENODEV;
   int ndev = 0;
@@ -145,6 +149,8 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   if (tc) {
     CK(C->tcA.ensure(tc_a_bytes(n)));
     CK(C->tcB.ensure(tc_b_bytes(n)));
+    CK(C->tcerr.ensure(2 * sizeof(int)));
+    CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
   }
   uint64_t* Lbuf = C->lbuf.as<uint64_t>();
   uint64_t* Ubuf = C->ubuf.as<uint64_t>();
@@ -221,11 +227,11 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       auto evp = take_events();
       cudaEventRecord(evp.first, st);
       if (tc) {
-        CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, Lbuf, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
-                              C->tcB.as<uint8_t>(), C->num_sms, st));
+        CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, n, Lbuf, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
+                              C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
         g_launches += 3;
       } else {
-        launch_trailing_plain<F>(f, R.m, ld, r0 + pb, n, jend, Lbuf, r0, Ubuf, n, pb, st);
+        launch_trailing_plain<F>(f, R.m, ld, r0 + pb, n, jend, n, Lbuf, r0, Ubuf, n, pb, st);
         g_launches++;
       }
       cudaEventRecord(evp.second, st);
@@ -240,6 +246,11 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
   }
   CK(cudaStreamSynchronize(st));
+  if (tc) {
+    int err = 0;
+    CK(cudaMemcpy(&err, C->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return MODLIN_ETIMEOUT;
+  }
   double tms = 0;
   for (size_t i = 0; i < ev_used; ++i) {
     float ms = 0;
@@ -299,6 +310,9 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
     g_launches++;
   } else {
     int ctas = opts && opts->grid_ctas > 0 ? opts->grid_ctas : C->num_sms;
+    // Each CTA keeps its slice of c in shared memory (<= 200 KiB).
+    const int64_t min_ctas = ((int64_t)n * 8 + 200 * 1024 - 1) / (200 * 1024);
+    if (ctas < min_ctas) ctas = (int)min_ctas;
     if ((int64_t)ctas > (int64_t)n) ctas = (int)n;
     CK(C->bmws.ensure((size_t)2 * n * 8));
     CK(C->bmsync.ensure(grid_sync_bytes()));
@@ -413,6 +427,43 @@ int modlin_rank_device(uint64_t p, uint64_t* d_m, size_t n, const modlin_rank_op
   std::lock_guard<std::mutex> g(C->mu);
   cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
   return rank_device_locked(C, p, d_m, n, opts, rank_out, pivot_cols_out, st, nullptr, nullptr);
+}
+
+int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t M, size_t N, const uint64_t* d_L,
+                                  const uint64_t* d_U, size_t ldu, size_t K, int kernel, void* stream) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (K > (size_t)kPanel || M > 0x3fffffff || N > 0x3fffffff || ldc < N || ldu < N) return MODLIN_EINVAL_N;
+  if ((M && N && K) && (!d_C || !d_L || !d_U)) return MODLIN_EINVAL_ARG;
+  if (!M || !N || !K) return MODLIN_OK;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  if (kernel == MODLIN_RANK_PLAIN) {
+    if (p == kM61)
+      launch_trailing_plain<FpM61>(FpM61(fp), d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U, (int64_t)ldu,
+                                   (int)K, st);
+    else
+      launch_trailing_plain<FpBarrett>(FpBarrett(fp), d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U,
+                                       (int64_t)ldu, (int)K, st);
+    g_launches++;
+    CK(cudaGetLastError());
+  } else {
+    CK(C->tcA.ensure(tc_a_bytes((int)M)));
+    CK(C->tcB.ensure(tc_b_bytes((int)N)));
+    CK(C->tcerr.ensure(2 * sizeof(int)));
+    CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
+    CK(launch_trailing_tc(fp, d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U, (int64_t)ldu, (int)K,
+                          C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
+    g_launches += 3;
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, C->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return MODLIN_ETIMEOUT;
+  }
+  return cuda_rc(cudaStreamSynchronize(st));
 }
 
 int modlin_rank_ex(uint64_t p, uint64_t* m, size_t n, const modlin_rank_opts* opts, size_t* rank_out,

@@ -251,7 +251,7 @@ __global__ void clear_pivot_flags_kernel(const PanelState* ps, uint8_t* is_pivot
 // ---------------------------------------------------------------------------
 template <class F>
 __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __restrict__ m, int64_t ld, int32_t rbeg,
-                                                              int32_t n, int32_t jend,
+                                                              int32_t n, int32_t jend, int32_t cend,
                                                               const uint64_t* __restrict__ Lbuf, int32_t r0,
                                                               const uint64_t* __restrict__ Ubuf, int64_t ldU,
                                                               int32_t K) {
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
     for (int idx = tid; idx < 64 * kc; idx += 256) {
       const int k = idx >> 6, ci = idx & 63;
       const int64_t c = ct + ci;
-      Us[k][ci] = c < n ? Ubuf[(int64_t)(k0 + k) * ldU + c] : 0;
+      Us[k][ci] = c < cend ? Ubuf[(int64_t)(k0 + k) * ldU + c] : 0;
     }
     __syncthreads();
     for (int k = 0; k < kc; ++k) {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int64_t c = ct + tx + 16 * q;
-      if (c < n) {
+      if (c < cend) {
         uint64_t* p = m + r * ld + c;
         *p = f.sub(*p, f.add(tot[i][q], f.reduce(acc[i][q])));
       }
@@ -372,11 +372,11 @@ void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st
 }
 
 template <class F>
-void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int n, int jend, const uint64_t* Lbuf,
-                           int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st) {
-  if (rbeg >= n || jend >= n || K <= 0) return;
-  dim3 grid((n - jend + 63) / 64, (n - rbeg + 63) / 64);
-  trailing_plain_kernel<F><<<grid, 256, 0, st>>>(f, m, ld, rbeg, n, jend, Lbuf, r0, Ubuf, ldU, K);
+void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st) {
+  if (rbeg >= rend || jend >= cend || K <= 0) return;
+  dim3 grid((cend - jend + 63) / 64, (rend - rbeg + 63) / 64);
+  trailing_plain_kernel<F><<<grid, 256, 0, st>>>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K);
 }
 
 #define INSTANTIATE(F)                                                                                          \
@@ -386,7 +386,7 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int n,
                                const uint64_t*, uint64_t*, const uint8_t*, int, cudaStream_t);                  \
   template void launch_couple<F>(const F&, const uint64_t*, int64_t, int, int, const PanelState*,               \
                                  const uint64_t*, uint64_t*, int64_t, cudaStream_t);                            \
-  template void launch_trailing_plain<F>(const F&, uint64_t*, int64_t, int, int, int, const uint64_t*, int,     \
+  template void launch_trailing_plain<F>(const F&, uint64_t*, int64_t, int, int, int, int, const uint64_t*, int, \
                                          const uint64_t*, int64_t, int, cudaStream_t);
 
 INSTANTIATE(FpBarrett)

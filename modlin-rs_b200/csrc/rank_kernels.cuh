@@ -23,7 +23,7 @@ void launch_moves(uint64_t* m, int64_t ld, int n, int jend, const int2* moves, i
                   int pb, cudaStream_t st);
 void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st);
 template <class F>
-void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int n, int jend, const uint64_t* Lbuf,
-                           int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st);
+void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st);
 
 }  // namespace modlin

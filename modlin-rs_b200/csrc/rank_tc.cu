@@ -1,19 +1,480 @@
-// Tensor-core trailing update — placeholder until the tcgen05 kernel lands:
-// MODLIN_RANK_TC reports "not supported" instead of silently running the
-// plain kernel.
-#include "rank_tc.cuh"
+// Exact modular trailing update on the 5th-generation tensor cores.
+//
+//   C[rbeg.., jend..] -= L * U  (mod p),   L: M x K,  U: K x N,  K = pb <= 64,
+//
+// the rank-pb update of the reference's blocked elimination
+// (src/fp.rs:202-248), recast as integer GEMMs that are exact:
+//
+// * Every residue x < p is split into LIMBS unsigned 8-bit limbs,
+//   x = sum_i 2^(8i) x_i (LIMBS = 1, 2, 4, 8 for p below 2^8, 2^16, 2^32,
+//   2^63). Then L*U = sum_d 2^(8d) S_d with S_d = sum_{i+j=d} L_i U_j.
+// * tcgen05.mma kind::i8 (u8 x u8 -> s32) computes the limb products. The B
+//   operand of one MMA is the LIMBS planes U_0..U_{LIMBS-1} of an NS-column
+//   subtile stacked along N (N = LIMBS*NS = 128); for plane i of L the MMA
+//   writes TMEM columns [i*NS, i*NS + 128), so the product L_i U_j lands in
+//   column block i+j: the diagonal sums S_d accumulate in TMEM for free.
+//   2*LIMBS-1 blocks of NS columns (240 of the 256 allocated for LIMBS = 8).
+// * No overflow: S_d <= LIMBS * K * 255^2 < 2^26 for K <= 64.
+// * Epilogue: T = sum_d 2^(8d) S_d reduced exactly mod p (for 2^61 - 1 the
+//   weights are powers of two mod p, so pairs of blocks fold into 32-bit
+//   words), then C = C - T mod p. Bit-exact against the u64 Barrett path.
+//
+// Operands are staged by cp.async.bulk (no tensor maps) in the canonical
+// K-major, no-swizzle UMMA layout: 8-row x 16-byte core matrices, LBO = 128 B
+// between the core matrices along K, SBO = 512 B between 8-row groups. The
+// limb planes are written to global memory in exactly that layout by the
+// split kernels, so each stage is one contiguous bulk copy.
+//
+// CTA = 6 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
+// the MMAs (one thread), warps 2-5 drain TMEM (warp w reads lanes
+// 32*(w%4)..+32). A CTA keeps its 128-row A tile (all limb planes) resident
+// and streams B subtiles through a 4-stage ring; two CTAs share an SM (256
+// TMEM columns each), so one CTA's epilogue overlaps the other's MMAs. Every
+// mbarrier wait is bounded; on expiry the kernel records an error, drains
+// its own copies and MMAs (bounded), frees TMEM and returns.
+#include <cuda_runtime.h>
 
 #include <climits>
+#include <cstdint>
+#include <type_traits>
+
+#include "field.cuh"
+#include "rank_tc.cuh"
 
 namespace modlin {
 
-int tc_crossover_n(uint64_t) { return INT_MAX; }
-size_t tc_a_bytes(int) { return 16; }
-size_t tc_b_bytes(int) { return 16; }
+namespace tc {
 
-cudaError_t launch_trailing_tc(const FieldParams&, uint64_t*, int64_t, int, int, int, const uint64_t*, int,
-                               const uint64_t*, int64_t, int, uint8_t*, uint8_t*, int, cudaStream_t) {
-  return cudaErrorNotSupported;
+constexpr int kK = 64;          // K (panel width) of one update, zero padded
+constexpr int kStages = 4;      // B ring depth
+constexpr int kTileBytes = 8192;  // one 128-row x 64-byte limb plane tile
+constexpr int kThreads = 192;
+constexpr uint32_t kTmemCols = 256;
+constexpr long long kSpinLimit = 4000000000LL;  // ~2 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait for the phase of `parity` to complete. false = gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kSpinLimit) return false;
+    if (*(volatile const int*)err) return false;
+  }
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle, LBO = 128 B (next
+// core matrix along K), SBO = sbo B (next 8-row group), version 1.
+__device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t sbo) {
+  const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
+  return a | (uint64_t(128 >> 4) << 16) | (uint64_t(sbo >> 4) << 32) | (1ULL << 46);
+}
+
+// Instruction descriptor: kind::i8, A = B = u8, D = s32, K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (uint32_t(n >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 16 consecutive 32-bit TMEM columns -> 16 registers per thread.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int LIMBS>
+struct Shape {
+  static constexpr int NS = 128 / LIMBS;             // output columns per subtile
+  static constexpr int DIAG = 2 * LIMBS - 1;         // diagonal accumulators
+  static constexpr int A_BYTES = LIMBS * kTileBytes;  // resident A tile
+  static constexpr int B_BYTES = kTileBytes;         // one B subtile (all planes)
+  static constexpr int ZERO_BYTES = 4096;            // zero A tile (128 x 32 B)
+  static constexpr int SMEM = A_BYTES + kStages * B_BYTES + ZERO_BYTES + 1024;
+};
+
+struct Sched {
+  int mtiles, nsub, chunk, nchunks;
+  __device__ __forceinline__ int units() const { return mtiles * nchunks; }
+};
+
+// ---------------------------------------------------------------------------
+// Limb split of L (A operand): Aw[mt][i][g][kc][rr][kb], thread per (row, kc).
+// ---------------------------------------------------------------------------
+template <int LIMBS>
+__global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int32_t r0, int32_t rbeg, int32_t rend, int32_t K,
+                               int32_t mpad, uint8_t* __restrict__ Aw) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)mpad * 4) return;
+  const int ri_all = (int)(idx >> 2), kc = (int)(idx & 3);
+  const int mt = ri_all >> 7, ri = ri_all & 127;
+  const int64_t r = (int64_t)rbeg + ri_all;
+  uint64_t v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int k = kc * 16 + q;
+    v[q] = (r < rend && k < K) ? Lbuf[(r - r0) * 64 + k] : 0;
+  }
+  const int64_t tile_off = ((int64_t)mt * LIMBS) * kTileBytes + (((ri >> 3) * 4 + kc) * 8 + (ri & 7)) * 16;
+#pragma unroll
+  for (int i = 0; i < LIMBS; ++i) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4) {
+      uint32_t x = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) x |= (uint32_t)((v[q4 * 4 + b] >> (8 * i)) & 0xFF) << (8 * b);
+      w[q4] = x;
+    }
+    *reinterpret_cast<uint4*>(Aw + tile_off + (int64_t)i * kTileBytes) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Limb split of U (B operand): Bw[sub][j][g2][kc][rr][kb], thread per
+// (column, kc); reads Ubuf[k][c] (coalesced over c).
+// ---------------------------------------------------------------------------
+template <int LIMBS>
+__global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, int32_t jend, int32_t cend, int32_t K,
+                               int32_t npad, uint8_t* __restrict__ Bw) {
+  constexpr int NS = Shape<LIMBS>::NS;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)npad * 4) return;
+  const int kc = (int)(idx / npad), ci = (int)(idx - (int64_t)kc * npad);
+  const int64_t c = (int64_t)jend + ci;
+  uint64_t v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int k = kc * 16 + q;
+    v[q] = (c < cend && k < K) ? Ubuf[(int64_t)k * ldU + c] : 0;
+  }
+  const int sub = ci / NS, cc = ci % NS;
+  const int64_t base = (int64_t)sub * kTileBytes + (((cc >> 3) * 4 + kc) * 8 + (cc & 7)) * 16;
+#pragma unroll
+  for (int j = 0; j < LIMBS; ++j) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4) {
+      uint32_t x = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) x |= (uint32_t)((v[q4 * 4 + b] >> (8 * j)) & 0xFF) << (8 * b);
+      w[q4] = x;
+    }
+    *reinterpret_cast<uint4*>(Bw + base + (int64_t)j * NS * kK) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Exact residue of sum_d 2^(8d) S_d for one output column (S in registers
+// acc_lo/acc_hi = the two 128-bit halves prepared by the fold).
+template <class F>
+__device__ __forceinline__ uint64_t finish(const F& f, u128 lo, u128 hi, uint64_t r64) {
+  if constexpr (std::is_same<F, FpM61>::value) {
+    return f.reduce(lo);  // already folded into one 128-bit value
+  } else {
+    return f.add(f.reduce(lo), f.mul(f.reduce(hi), r64));
+  }
+}
+
+template <class F, int LIMBS>
+__global__ void __launch_bounds__(kThreads, 2)
+    trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
+                       int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err) {
+  using SH = Shape<LIMBS>;
+  constexpr int NS = SH::NS;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sA = smem;                                          // A_BYTES
+  uint8_t* sB = smem + SH::A_BYTES;                            // kStages * 8 KB
+  uint8_t* sZ = sB + kStages * SH::B_BYTES;                    // 4 KB of zeros
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES);
+  uint64_t* a_full = bars + 0;
+  uint64_t* a_empty = bars + 1;
+  uint64_t* acc_full = bars + 2;
+  uint64_t* acc_empty = bars + 3;
+  uint64_t* mma_done = bars + 4;
+  uint64_t* b_full = bars + 8;
+  uint64_t* b_empty = bars + 8 + kStages;
+  __shared__ uint32_t tmem_base_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < SH::ZERO_BYTES / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(sZ)[i] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    mbar_init(a_full, 1);
+    mbar_init(a_empty, 1);
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 4);
+    mbar_init(mma_done, 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(b_full + s, 1);
+      mbar_init(b_empty + s, 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // Make the zero tile visible to the tensor core (async proxy).
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const int units = S.units();
+
+  if (warp == 0) {
+    // ---------------- producer: bulk copies -------------------------------
+    if (lane == 0) {
+      int it = 0, u_local = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++u_local) {
+        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
+        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+        if (u_local > 0 && !(ok = mbar_wait(a_empty, (u_local - 1) & 1, err))) break;
+        mbar_arrive_expect_tx(a_full, SH::A_BYTES);
+        bulk_g2s(sA, Aw + (int64_t)mt * SH::A_BYTES, SH::A_BYTES, a_full);
+        for (int s = s0; s < s1; ++s, ++it) {
+          const int st = it % kStages;
+          if (it >= kStages && !(ok = mbar_wait(b_empty + st, ((it / kStages) - 1) & 1, err))) break;
+          mbar_arrive_expect_tx(b_full + st, SH::B_BYTES);
+          bulk_g2s(sB + st * SH::B_BYTES, Bw + (int64_t)s * SH::B_BYTES, SH::B_BYTES, b_full + st);
+        }
+      }
+      if (!ok) {
+        atomicExch(err, 1);
+        // Let this CTA's own copies land before the CTA can exit.
+        for (int st = 0; st < kStages; ++st)
+          if (it > st) mbar_wait(b_full + st, ((it - 1 - st) / kStages) & 1, err + 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ------------------------------------------
+    if (lane == 0) {
+      int it = 0, u_local = 0;
+      bool ok = true;
+      const uint32_t id_full = idesc_i8(LIMBS * NS);
+      const uint32_t id_zero = idesc_i8(LIMBS > 1 ? (LIMBS - 1) * NS : 16);
+      for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++u_local) {
+        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
+        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+        (void)mt;
+        if (!(ok = mbar_wait(a_full, u_local & 1, err))) break;
+        fence_after();
+        for (int s = s0; s < s1; ++s, ++it) {
+          const int st = it % kStages;
+          if (it > 0 && !(ok = mbar_wait(acc_empty, (it - 1) & 1, err))) break;
+          if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+          fence_after();
+          const uint8_t* bt = sB + st * SH::B_BYTES;
+          if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
+            mma_i8(tmem + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
+#pragma unroll
+          for (int i = 0; i < LIMBS; ++i)
+#pragma unroll
+            for (int ks = 0; ks < kK / 32; ++ks)
+              mma_i8(tmem + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
+                     id_full, (i > 0 || ks > 0) ? 1u : 0u);
+          mma_commit(b_empty + st);
+          mma_commit(acc_full);
+        }
+        if (ok) mma_commit(a_empty);
+      }
+      if (!ok) atomicExch(err, 1);
+      mma_commit(mma_done);
+      mbar_wait(mma_done, 0, err + 1);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: TMEM -> exact residue -> C -= T -------------
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
+    int it = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+      const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
+      const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+      const int64_t r = (int64_t)rbeg + (int64_t)mt * 128 + row;
+      for (int s = s0; s < s1; ++s, ++it) {
+        ok = __all_sync(0xffffffffu, mbar_wait(acc_full, it & 1, err));
+        if (!ok) break;
+        fence_after();
+        for (int q = 0; q < NS / 16; ++q) {
+          u128 lo[16], hi[16];
+#pragma unroll
+          for (int c = 0; c < 16; ++c) lo[c] = hi[c] = 0;
+          if constexpr (std::is_same<F, FpM61>::value && LIMBS == 8) {
+            // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: fold block d+8 into d.
+#pragma unroll
+            for (int d = 0; d < 15; ++d) {
+              uint32_t a[16];
+              tmem_ld16(lane_addr + d * NS + q * 16, a);
+              tmem_wait_ld();
+              const int sh = d < 8 ? 8 * d : 8 * (d - 8) + 3;
+#pragma unroll
+              for (int c = 0; c < 16; ++c) lo[c] += (u128)a[c] << sh;
+            }
+          } else {
+#pragma unroll 1
+            for (int d = 0; d < SH::DIAG; ++d) {
+              uint32_t a[16];
+              tmem_ld16(lane_addr + d * NS + q * 16, a);
+              tmem_wait_ld();
+#pragma unroll
+              for (int c = 0; c < 16; ++c) {
+                if (d < 8)
+                  lo[c] += (u128)a[c] << (8 * d);
+                else
+                  hi[c] += (u128)a[c] << (8 * (d - 8));
+              }
+            }
+          }
+          if (q == NS / 16 - 1) {
+            // All accumulator reads done: hand TMEM back to the MMA warp.
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty);
+          }
+          if (r < rend) {
+            const int64_t c0 = (int64_t)jend + (int64_t)s * NS + q * 16;
+            uint64_t* crow = m + r * ld + c0;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+              if (c0 + c < cend) {
+                const uint64_t t = finish(f, lo[c], hi[c], r64);
+                crow[c] = f.sub(crow[c], t);
+              }
+            }
+          }
+        }
+      }
+    }
+    if (!ok) atomicExch(err, 1);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+int limbs_for(uint64_t p) {
+  const int bits = 64 - __builtin_clzll(p - 1);
+  return bits <= 8 ? 1 : bits <= 16 ? 2 : bits <= 32 ? 4 : 8;
+}
+
+template <class F, int LIMBS>
+cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint64_t* Lbuf, int r0,
+                     const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw, uint8_t* Bw, int num_sms, uint64_t r64,
+                     int* err, cudaStream_t st) {
+  using SH = Shape<LIMBS>;
+  const int M = rend - rbeg, N = cend - jend;
+  const int mtiles = (M + 127) / 128, nsub = (N + SH::NS - 1) / SH::NS;
+  const int mpad = mtiles * 128, npad = nsub * SH::NS;
+  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(Lbuf, r0, rbeg, rend, K, mpad, Aw);
+  split_b_kernel<LIMBS><<<(npad * 4 + 255) / 256, 256, 0, st>>>(Ubuf, ldU, jend, cend, K, npad, Bw);
+  Sched S;
+  S.mtiles = mtiles;
+  S.nsub = nsub;
+  const int ctas = 2 * num_sms;
+  // Chunk the N subtiles so that there are >= ~2 units per CTA when possible.
+  int chunk = nsub;
+  while (chunk > 8 && (int64_t)mtiles * ((nsub + chunk - 1) / chunk) < 2 * ctas) chunk = (chunk + 1) / 2;
+  S.chunk = chunk;
+  S.nchunks = (nsub + chunk - 1) / chunk;
+  const int units = S.mtiles * S.nchunks;
+  const int grid = units < ctas ? units : ctas;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
+    attr = true;
+  }
+  trailing_tc_kernel<F, LIMBS><<<grid, kThreads, SH::SMEM, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64, err);
+  return cudaGetLastError();
+}
+
+}  // namespace tc
+
+int tc_crossover_n(uint64_t) { return 512; }
+
+size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc::kK * 8; }
+size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kK * 8; }
+
+cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+                               const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw,
+                               uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
+  if (rbeg >= rend || jend >= cend || K <= 0) return cudaSuccess;
+  if (K > tc::kK) return cudaErrorInvalidValue;
+  const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
+  const int L = tc::limbs_for(fp.p);
+  if (fp.p == kM61)
+    return tc::launch_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err,
+                                  st);
+  const FpBarrett f(fp);
+  switch (L) {
+    case 1: return tc::launch_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    case 2: return tc::launch_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    case 4: return tc::launch_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    default: return tc::launch_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+  }
 }
 
 }  // namespace modlin

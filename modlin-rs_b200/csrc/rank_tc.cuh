@@ -12,11 +12,14 @@ namespace modlin {
 // Smallest side for which MODLIN_RANK_AUTO uses the tensor-core update.
 int tc_crossover_n(uint64_t p);
 // Workspace bytes for the limb planes of L (rows x K) and U (K x cols).
-size_t tc_a_bytes(int n);
-size_t tc_b_bytes(int n);
-// A[rbeg.., jend..] -= L * U mod p via exact INT8-limb GEMMs.
-cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int n, int jend,
+size_t tc_a_bytes(int rows);
+size_t tc_b_bytes(int cols);
+// A[rbeg..rend, jend..cend] -= L * U mod p via exact INT8-limb GEMMs (L row
+// r at Lbuf[(r - r0) * 64], U row k at Ubuf[k * ldU], absolute columns). `err` points
+// at two device ints (zeroed by the caller); err[0] != 0 afterwards means a
+// bounded wait inside the kernel expired.
+cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
                                const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw,
-                               uint8_t* Bw, int num_sms, cudaStream_t st);
+                               uint8_t* Bw, int num_sms, int* err, cudaStream_t st);
 
 }  // namespace modlin

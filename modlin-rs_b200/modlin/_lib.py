@@ -71,6 +71,7 @@ def lib():
     _proto(L, "modlin_rank", ci, [u64, u64p, szt, sztp, PROGRESS, vp])
     _proto(L, "modlin_rank_ex", ci, [u64, u64p, szt, ctypes.POINTER(RankOpts), sztp, sztp, PROGRESS, vp])
     _proto(L, "modlin_rank_device", ci, [u64, vp, szt, ctypes.POINTER(RankOpts), sztp, sztp, vp])
+    _proto(L, "modlin_trailing_update_device", ci, [u64, vp, szt, szt, szt, vp, vp, szt, szt, ci, vp])
     _proto(L, "modlin_linear_complexity", ci, [u64, u64p, szt, sztp, PROGRESS, vp])
     _proto(L, "modlin_linear_complexity_ex", ci, [u64, u64p, szt, ctypes.POINTER(LcOpts), sztp])
     _proto(L, "modlin_linear_complexity_device", ci, [u64, vp, szt, ctypes.POINTER(LcOpts), sztp, vp])
@@ -102,7 +103,7 @@ def check(rc: int, what: str = "") -> None:
 # Names every build of the library must export (include/modlin.h).
 EXPORTED = [
     "modlin_strerror", "modlin_field_new", "modlin_field_reduce", "modlin_field_reduce_u128",
-    "modlin_field_mul", "modlin_rank", "modlin_rank_ex", "modlin_rank_device",
+    "modlin_field_mul", "modlin_rank", "modlin_rank_ex", "modlin_rank_device", "modlin_trailing_update_device",
     "modlin_linear_complexity", "modlin_linear_complexity_ex", "modlin_linear_complexity_device",
     "modlin_rank_batch", "modlin_lc_batch", "modlin_lc_batch_device", "modlin_corank_prob",
     "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue", "modlin_pretty_p_value",

@@ -146,3 +146,11 @@ def lc_batch_device(ps, ptrs, ns, stream: int = 0) -> list[int]:
     out = (szt * k)()
     check(lib().modlin_lc_batch_device(P, D, N, k, out, stream or None), "lc_batch_device")
     return [int(out[i]) for i in range(k)]
+
+
+def trailing_update_device(field, c_ptr: int, ldc: int, M: int, N: int, l_ptr: int, u_ptr: int, ldu: int, K: int,
+                           *, kernel: str = "tc", stream: int = 0) -> None:
+    """C[M x N] -= L[M x K] * U[K x N] mod p on device buffers (L row stride 64)."""
+    rc = lib().modlin_trailing_update_device(_p(field), c_ptr, ldc, M, N, l_ptr, u_ptr, ldu, K, KERNELS[kernel],
+                                             stream or None)
+    check(rc, "trailing_update_device")

@@ -18,7 +18,7 @@ KERNELS = ["plain", "tc"]
 def kernels_available(M):
     ks = ["plain"]
     try:
-        M.rank(M61, np.eye(2, dtype=np.uint64), 2, kernel="tc")
+        M.rank(M61, np.eye(130, dtype=np.uint64), 130, kernel="tc")
         ks.append("tc")
     except M.ModlinError:
         pass

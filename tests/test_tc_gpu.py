@@ -1,0 +1,66 @@
+"""The tensor-core trailing update (tcgen05 kind::i8 limb GEMMs) on its own:
+C -= L*U mod p through the C ABI, compared with exact Python integers and
+with the u64 Barrett kernel, for every limb count (1, 2, 4, 8 limbs)."""
+import numpy as np
+import pytest
+
+from conftest import M61
+
+pytestmark = pytest.mark.gpu
+
+PRIMES = [127, 251, 65521, 2147483647, 4294967291, M61, (1 << 62) + 135, (1 << 63) - 25]
+
+
+def rand_res(rng, p, shape):
+    return (rng.integers(0, 2**63, shape, dtype=np.uint64) % np.uint64(p)).astype(np.uint64)
+
+
+def run(M, p, C, L, U, kernel):
+    import torch
+    Mr, N = C.shape
+    K = U.shape[0]
+    Lp = np.zeros((Mr, 64), dtype=np.uint64)
+    Lp[:, :K] = L
+    dC = torch.from_numpy(C.view(np.int64).copy()).cuda()
+    dL = torch.from_numpy(Lp.view(np.int64).copy()).cuda()
+    dU = torch.from_numpy(np.ascontiguousarray(U).view(np.int64).copy()).cuda()
+    M.fp.trailing_update_device(p, dC.data_ptr(), N, Mr, N, dL.data_ptr(), dU.data_ptr(), N, K, kernel=kernel)
+    torch.cuda.synchronize()
+    return dC.cpu().numpy().view(np.uint64)
+
+
+def exact(p, C, L, U):
+    Co = C.astype(object)
+    prod = L.astype(object).dot(U.astype(object))
+    return ((Co - prod) % p).astype(np.uint64)
+
+
+@pytest.mark.parametrize("p", PRIMES)
+def test_small_exact(M, p):
+    rng = np.random.default_rng(p % 1000)
+    for Mr, N, K in [(128, 16, 64), (130, 70, 64), (5, 3, 1), (200, 129, 33)]:
+        C, L, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
+        want = exact(p, C, L, U)
+        assert np.array_equal(run(M, p, C, L, U, "plain"), want), (p, Mr, N, K, "plain")
+        assert np.array_equal(run(M, p, C, L, U, "tc"), want), (p, Mr, N, K, "tc")
+
+
+@pytest.mark.parametrize("p", PRIMES)
+def test_extreme_values(M, p):
+    """All entries p-1: the largest limb products and accumulator sums."""
+    for Mr, N, K in [(256, 256, 64), (129, 33, 64)]:
+        C = np.full((Mr, N), p - 1, dtype=np.uint64)
+        L = np.full((Mr, K), p - 1, dtype=np.uint64)
+        U = np.full((K, N), p - 1, dtype=np.uint64)
+        want = exact(p, C[:4, :4], L[:4], U[:, :4])
+        got = run(M, p, C, L, U, "tc")
+        assert np.array_equal(got[:4, :4], want)
+        assert np.array_equal(got, run(M, p, C, L, U, "plain"))
+
+
+@pytest.mark.parametrize("p", [M61, 2147483647, 65521, 127, (1 << 63) - 25])
+def test_large_tc_equals_plain(M, p):
+    rng = np.random.default_rng(7)
+    for Mr, N, K in [(2048, 1536, 64), (1000, 3001, 17), (4096, 512, 64)]:
+        C, L, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
+        assert np.array_equal(run(M, p, C, L, U, "tc"), run(M, p, C, L, U, "plain")), (p, Mr, N, K)
