@@ -121,6 +121,19 @@ int modlin_linear_complexity_ex(uint64_t p, const uint64_t *s, size_t n, const m
 int modlin_linear_complexity_device(uint64_t p, const uint64_t *d_s, size_t n,
                                     const modlin_lc_opts *opts, size_t *lc_out, void *stream);
 
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory on the call path (a host whose pool allocator owns all device
+ * memory, or a loop that must not pay cudaMalloc's implicit synchronisation):
+ * the linear complexity of the device sequence d_s[0..n) is written to the
+ * device slot *d_lc_out, asynchronously on `stream`, without any allocation.
+ * The Berlekamp-Massey scratch lives in a fixed 6 MiB device array, so
+ * n <= 262144 (MODLIN_EINVAL_N beyond). All calls share that array: calls
+ * that overlap on the GPU race, so order them (e.g. one stream). The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture. */
+int modlin_linear_complexity_device_noalloc(uint64_t p, const uint64_t *d_s, size_t n,
+                                            int64_t *d_lc_out, void *stream);
+
 /* ---- Batched jobs (the CLI's `reps`, src/main.rs:82 and :152) ----------- */
 
 typedef struct {
