@@ -183,13 +183,16 @@ __global__ void __launch_bounds__(256) bulk_kernel(F f, uint64_t* __restrict__ m
 // ---------------------------------------------------------------------------
 // couple_kernel — U block (src/fp.rs:184-200): for every trailing column c,
 // U_k[c] = alpha_k * row_{prow_k}[c] - sum_{k2<k} G[k][k2] * U_k2[c],
-// sequential in k, a thread per column, u128 lazy accumulation.
+// sequential in k, a thread per column; the column's coupled values stay in
+// registers (fully unrolled triangular loop), u128 lazy accumulation.
 // ---------------------------------------------------------------------------
 template <class F>
-__global__ void __launch_bounds__(256) couple_kernel(F f, const uint64_t* __restrict__ m, int64_t ld, int32_t n,
+__global__ void __launch_bounds__(128) couple_kernel(F f, const uint64_t* __restrict__ m, int64_t ld, int32_t n,
                                                       int32_t jend, const PanelState* __restrict__ ps,
                                                       const uint64_t* __restrict__ G, uint64_t* Ubuf, int64_t ldU) {
-  __shared__ uint64_t Gs[kPanel][kPanel + 1];
+  extern __shared__ __align__(16) uint64_t smem_c[];
+  uint64_t(*Us)[128] = reinterpret_cast<uint64_t(*)[128]>(smem_c);            // [64][128]: my column's U_k
+  uint64_t(*Gs)[kPanel] = reinterpret_cast<uint64_t(*)[kPanel]>(smem_c + kPanel * 128);  // [64][64]
   __shared__ uint64_t al[kPanel];
   __shared__ int32_t prs[kPanel];
   const int pb = ps->pb;
@@ -199,26 +202,26 @@ __global__ void __launch_bounds__(256) couple_kernel(F f, const uint64_t* __rest
     prs[k] = ps->prow[k];
   }
   __syncthreads();
-  const int64_t c = (int64_t)jend + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
+  const int t = threadIdx.x;
+  const int64_t c = (int64_t)jend + (int64_t)blockIdx.x * blockDim.x + t;
+  const bool valid = c < n;
   const uint64_t sb = f.safe_batch();
   for (int k = 0; k < pb; ++k) {
-    const uint64_t v = f.mul(al[k], m[(int64_t)prs[k] * ld + c]);
+    const uint64_t v = valid ? f.mul(al[k], m[(int64_t)prs[k] * ld + c]) : 0;
     u128 acc = 0;
     uint64_t tot = 0, cnt = 0;
+#pragma unroll 8
     for (int k2 = 0; k2 < k; ++k2) {
-      const uint64_t g = Gs[k][k2];
-      if (g) {
-        acc += (u128)g * Ubuf[(int64_t)k2 * ldU + c];
-        if (++cnt == sb) {
-          tot = f.add(tot, f.reduce(acc));
-          acc = 0;
-          cnt = 0;
-        }
+      acc += (u128)Gs[k][k2] * Us[k2][t];
+      if (++cnt == sb) {
+        tot = f.add(tot, f.reduce(acc));
+        acc = 0;
+        cnt = 0;
       }
     }
-    tot = f.add(tot, f.reduce(acc));
-    Ubuf[(int64_t)k * ldU + c] = f.sub(v, tot);
+    const uint64_t u = f.sub(v, f.add(tot, f.reduce(acc)));
+    Us[k][t] = u;
+    if (valid) Ubuf[(int64_t)k * ldU + c] = u;
   }
 }
 
@@ -354,7 +357,13 @@ template <class F>
 void launch_couple(const F& f, const uint64_t* m, int64_t ld, int n, int jend, const PanelState* ps,
                    const uint64_t* G, uint64_t* Ubuf, int64_t ldU, cudaStream_t st) {
   const int cols = n - jend;
-  couple_kernel<F><<<(cols + 255) / 256, 256, 0, st>>>(f, m, ld, n, jend, ps, G, Ubuf, ldU);
+  const size_t smem = (size_t)(kPanel * 128 + kPanel * kPanel) * sizeof(uint64_t);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(couple_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  couple_kernel<F><<<(cols + 127) / 128, 128, smem, st>>>(f, m, ld, n, jend, ps, G, Ubuf, ldU);
 }
 
 void launch_moves(uint64_t* m, int64_t ld, int n, int jend, const int2* moves, int nmoves, uint64_t* Lbuf, int r0,

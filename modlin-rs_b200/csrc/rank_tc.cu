@@ -25,9 +25,9 @@
 // limb planes are written to global memory in exactly that layout by the
 // split kernels, so each stage is one contiguous bulk copy.
 //
-// CTA = 6 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
-// the MMAs (one thread), warps 2-5 drain TMEM (warp w reads lanes
-// 32*(w%4)..+32). A CTA keeps its 128-row A tile (all limb planes) resident
+// CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
+// the MMAs (one thread), warps 2-9 drain TMEM (warp w reads lanes
+// 32*(w%4)..+32, 8 of every 16 columns). A CTA keeps its 128-row A tile (all limb planes) resident
 // and streams B subtiles through a 4-stage ring; two CTAs share an SM (256
 // TMEM columns each), so one CTA's epilogue overlaps the other's MMAs. Every
 // mbarrier wait is bounded; on expiry the kernel records an error, drains
@@ -48,7 +48,7 @@ namespace tc {
 constexpr int kK = 64;          // K (panel width) of one update, zero padded
 constexpr int kStages = 4;      // B ring depth
 constexpr int kTileBytes = 8192;  // one 128-row x 64-byte limb plane tile
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
 constexpr uint32_t kTmemCols = 256;
 constexpr long long kSpinLimit = 4000000000LL;  // ~2 s at 2 GHz
 
@@ -134,6 +134,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr)
       : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit TMEM columns -> 8 registers per thread.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_init(a_full, 1);
     mbar_init(a_empty, 1);
     mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 4);
+    mbar_init(acc_empty, 8);
     mbar_init(mma_done, 1);
     for (int s = 0; s < kStages; ++s) {
       mbar_init(b_full + s, 1);
@@ -343,42 +351,58 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncwarp();
   } else {
     // ---------------- epilogue: TMEM -> exact residue -> C -= T -------------
+    // 8 warps: warp w reads TMEM lanes 32*(w%4)..+32 (its rows) and the
+    // 8-column half (w-2)/4 of every 16-column chunk. The row's C segment is
+    // loaded before waiting for the MMA, so DRAM latency overlaps it.
     const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = quad * 32 + lane;
-    const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + half * 8;
     int it = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
       const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
       const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
       const int64_t r = (int64_t)rbeg + (int64_t)mt * 128 + row;
+      const bool row_ok = r < rend;
       for (int s = s0; s < s1; ++s, ++it) {
+        uint64_t cv[8];
+        int64_t c0 = (int64_t)jend + (int64_t)s * NS + half * 8;
+        uint64_t* crow = m + r * ld + c0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
         ok = __all_sync(0xffffffffu, mbar_wait(acc_full, it & 1, err));
         if (!ok) break;
         fence_after();
         for (int q = 0; q < NS / 16; ++q) {
-          u128 lo[16], hi[16];
+          if (q > 0) {
+            c0 = (int64_t)jend + (int64_t)s * NS + q * 16 + half * 8;
+            crow = m + r * ld + c0;
 #pragma unroll
-          for (int c = 0; c < 16; ++c) lo[c] = hi[c] = 0;
+            for (int c = 0; c < 8; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
+          }
+          u128 lo[8], hi[8];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
           if constexpr (std::is_same<F, FpM61>::value && LIMBS == 8) {
             // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: fold block d+8 into d.
 #pragma unroll
             for (int d = 0; d < 15; ++d) {
-              uint32_t a[16];
-              tmem_ld16(lane_addr + d * NS + q * 16, a);
+              uint32_t a[8];
+              tmem_ld8(lane_addr + d * NS + q * 16, a);
               tmem_wait_ld();
               const int sh = d < 8 ? 8 * d : 8 * (d - 8) + 3;
 #pragma unroll
-              for (int c = 0; c < 16; ++c) lo[c] += (u128)a[c] << sh;
+              for (int c = 0; c < 8; ++c) lo[c] += (u128)a[c] << sh;
             }
           } else {
 #pragma unroll 1
             for (int d = 0; d < SH::DIAG; ++d) {
-              uint32_t a[16];
-              tmem_ld16(lane_addr + d * NS + q * 16, a);
+              uint32_t a[8];
+              tmem_ld8(lane_addr + d * NS + q * 16, a);
               tmem_wait_ld();
 #pragma unroll
-              for (int c = 0; c < 16; ++c) {
+              for (int c = 0; c < 8; ++c) {
                 if (d < 8)
                   lo[c] += (u128)a[c] << (8 * d);
                 else
@@ -392,16 +416,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             __syncwarp();
             if (lane == 0) mbar_arrive(acc_empty);
           }
-          if (r < rend) {
-            const int64_t c0 = (int64_t)jend + (int64_t)s * NS + q * 16;
-            uint64_t* crow = m + r * ld + c0;
+          if (row_ok) {
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
-              if (c0 + c < cend) {
-                const uint64_t t = finish(f, lo[c], hi[c], r64);
-                crow[c] = f.sub(crow[c], t);
-              }
-            }
+            for (int c = 0; c < 8; ++c)
+              if (c0 + c < cend) crow[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
           }
         }
       }
