@@ -28,8 +28,9 @@
 // CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
 // the MMAs (one thread), warps 2-9 drain TMEM (warp w reads lanes
 // 32*(w%4)..+32, 8 of every 16 columns). A CTA keeps its 128-row A tile (all limb planes) resident
-// and streams B subtiles through a 4-stage ring; two CTAs share an SM (256
-// TMEM columns each), so one CTA's epilogue overlaps the other's MMAs. Every
+// and streams B subtiles through a 6-stage ring; one CTA per SM owns all 512
+// TMEM columns as two accumulator buffers, so the MMAs of subtile s+1 run
+// while the epilogue drains subtile s. Every
 // mbarrier wait is bounded; on expiry the kernel records an error, drains
 // its own copies and MMAs (bounded), frees TMEM and returns.
 #include <cuda_runtime.h>
@@ -46,10 +47,12 @@ namespace modlin {
 namespace tc {
 
 constexpr int kK = 64;          // K (panel width) of one update, zero padded
-constexpr int kStages = 4;      // B ring depth
+constexpr int kStages = 6;      // B ring depth
 constexpr int kTileBytes = 8192;  // one 128-row x 64-byte limb plane tile
 constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // two accumulator buffers of 256 columns
+constexpr int kCDepth = 4;           // staged C tiles (subtiles) in shared memory
+constexpr int kCStride = 17;         // padded row stride (words) of a staged 128 x 16 C tile
 constexpr long long kSpinLimit = 4000000000LL;  // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -144,6 +147,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
                : "memory");
 }
 
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 template <int LIMBS>
@@ -153,7 +165,8 @@ struct Shape {
   static constexpr int A_BYTES = LIMBS * kTileBytes;  // resident A tile
   static constexpr int B_BYTES = kTileBytes;         // one B subtile (all planes)
   static constexpr int ZERO_BYTES = 4096;            // zero A tile (128 x 32 B)
-  static constexpr int SMEM = A_BYTES + kStages * B_BYTES + ZERO_BYTES + 1024;
+  static constexpr int C_BYTES = LIMBS == 8 ? kCDepth * 128 * kCStride * 8 : 0;  // staged C tiles
+  static constexpr int SMEM = A_BYTES + kStages * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
 };
 
 struct Sched {
@@ -239,7 +252,7 @@ __device__ __forceinline__ uint64_t finish(const F& f, u128 lo, u128 hi, uint64_
 }
 
 template <class F, int LIMBS>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
                        int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err) {
   using SH = Shape<LIMBS>;
@@ -249,11 +262,12 @@ __global__ void __launch_bounds__(kThreads, 2)
   uint8_t* sB = smem + SH::A_BYTES;                            // kStages * 8 KB
   uint8_t* sZ = sB + kStages * SH::B_BYTES;                    // 4 KB of zeros
   uint64_t* bars = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES);
+  uint64_t* sC = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024);  // [kCDepth][128][kCStride]
   uint64_t* a_full = bars + 0;
   uint64_t* a_empty = bars + 1;
-  uint64_t* acc_full = bars + 2;
-  uint64_t* acc_empty = bars + 3;
-  uint64_t* mma_done = bars + 4;
+  uint64_t* acc_full = bars + 2;   // [2]: accumulator buffer b holds a finished subtile
+  uint64_t* acc_empty = bars + 4;  // [2]: the epilogue has drained buffer b
+  uint64_t* mma_done = bars + 6;
   uint64_t* b_full = bars + 8;
   uint64_t* b_empty = bars + 8 + kStages;
   __shared__ uint32_t tmem_base_sh;
@@ -264,8 +278,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (threadIdx.x == 0) {
     mbar_init(a_full, 1);
     mbar_init(a_empty, 1);
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 8);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + b, 1);
+      mbar_init(acc_empty + b, 8);
+    }
     mbar_init(mma_done, 1);
     for (int s = 0; s < kStages; ++s) {
       mbar_init(b_full + s, 1);
@@ -327,20 +343,22 @@ __global__ void __launch_bounds__(kThreads, 2)
         fence_after();
         for (int s = s0; s < s1; ++s, ++it) {
           const int st = it % kStages;
-          if (it > 0 && !(ok = mbar_wait(acc_empty, (it - 1) & 1, err))) break;
+          const int ab = it & 1;  // accumulator buffer
+          if (it >= 2 && !(ok = mbar_wait(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
           if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
           fence_after();
           const uint8_t* bt = sB + st * SH::B_BYTES;
+          const uint32_t dacc = tmem + ab * 256;
           if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
-            mma_i8(tmem + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
+            mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
 #pragma unroll
           for (int i = 0; i < LIMBS; ++i)
 #pragma unroll
             for (int ks = 0; ks < kK / 32; ++ks)
-              mma_i8(tmem + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
+              mma_i8(dacc + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
                      id_full, (i > 0 || ks > 0) ? 1u : 0u);
           mma_commit(b_empty + st);
-          mma_commit(acc_full);
+          mma_commit(acc_full + ab);
         }
         if (ok) mma_commit(a_empty);
       }
@@ -352,50 +370,166 @@ __global__ void __launch_bounds__(kThreads, 2)
   } else {
     // ---------------- epilogue: TMEM -> exact residue -> C -= T -------------
     // 8 warps: warp w reads TMEM lanes 32*(w%4)..+32 (its rows) and the
-    // 8-column half (w-2)/4 of every 16-column chunk. The row's C segment is
-    // loaded before waiting for the MMA, so DRAM latency overlaps it.
+    // 8-column half (w-2)/4 of every 16-column chunk; the accumulator buffer
+    // is released as soon as its columns are in registers.
     const int quad = warp & 3;
     const int half = (warp - 2) >> 2;
     const int row = quad * 32 + lane;
-    const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + half * 8;
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + half * 8;
     int it = 0;
     bool ok = true;
-    for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
-      const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
-      const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
-      const int64_t r = (int64_t)rbeg + (int64_t)mt * 128 + row;
-      const bool row_ok = r < rend;
-      for (int s = s0; s < s1; ++s, ++it) {
-        uint64_t cv[8];
-        int64_t c0 = (int64_t)jend + (int64_t)s * NS + half * 8;
-        uint64_t* crow = m + r * ld + c0;
+    if constexpr (LIMBS == 8) {
+      // C goes through shared memory so that global accesses are coalesced:
+      // warp w copies rows 16(w-2)..+16 of the 128 x 16 tile (two 128-byte
+      // rows per instruction) kCDepth - 1 subtiles ahead with cp.async, every
+      // thread then works on its own row in shared memory, and the results
+      // leave the same way. Named barrier 1 synchronises the 8 epilogue warps.
+      const int ew = warp - 2, rr = lane >> 4, cc = lane & 15;
+      auto epi_bar = []() { asm volatile("bar.sync 1, 256;" ::: "memory"); };
+      int pu = blockIdx.x, ps = 0, ps1 = 0, pcount = 0;
+      int64_t pbase = 0;
+      auto pf_unit = [&]() {
+        if (pu < units) {
+          const int mt = pu / S.nchunks, ch = pu - mt * S.nchunks;
+          ps = ch * S.chunk;
+          ps1 = min(S.nsub, ps + S.chunk);
+          pbase = (int64_t)rbeg + (int64_t)mt * 128;
+        }
+      };
+      auto pf_issue = [&]() {
+        if (pu < units) {
+          uint64_t* slot = sC + (size_t)(pcount % kCDepth) * 128 * kCStride;
+          const int64_t gc = (int64_t)jend + (int64_t)ps * NS + cc;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
-        ok = __all_sync(0xffffffffu, mbar_wait(acc_full, it & 1, err));
-        if (!ok) break;
-        fence_after();
-        for (int q = 0; q < NS / 16; ++q) {
-          if (q > 0) {
-            c0 = (int64_t)jend + (int64_t)s * NS + q * 16 + half * 8;
-            crow = m + r * ld + c0;
+          for (int i = 0; i < 8; ++i) {
+            const int lr = ew * 16 + 2 * i + rr;
+            const int64_t gr = pbase + lr;
+            if (gr < rend && gc < cend) cp_async8(slot + lr * kCStride + cc, m + gr * ld + gc);
+          }
+          if (++ps == ps1) {
+            pu += gridDim.x;
+            pf_unit();
+          }
+        }
+        cp_async_commit();
+        ++pcount;
+      };
+      pf_unit();
+      for (int k = 0; k < kCDepth - 1; ++k) pf_issue();
+      for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
+        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+        const int64_t base = (int64_t)rbeg + (int64_t)mt * 128;
+        const bool row_ok = base + row < rend;
+        for (int s = s0; s < s1; ++s, ++it) {
+          const int ab = it & 1;
+          const uint32_t lane_addr = lane_base + ab * 256;
+          cp_async_wait<kCDepth - 2>();
+          epi_bar();  // this subtile's C is in shared memory; the previous one has been stored
+          pf_issue();
+          uint64_t* slot = sC + (size_t)(it % kCDepth) * 128 * kCStride;
+          uint64_t* my = slot + row * kCStride + half * 8;
+          const int64_t c0 = (int64_t)jend + (int64_t)s * NS + half * 8;
+          uint64_t cv[8];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) cv[c] = my[c];
+          if (ok) ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
+          if (ok) {
+            fence_after();
+            uint64_t res[8];
+            if constexpr (std::is_same<F, FpM61>::value) {
+              uint32_t a[15][8];
+#pragma unroll
+              for (int d = 0; d < 15; ++d) tmem_ld8(lane_addr + d * NS, a[d]);
+              tmem_wait_ld();
+#pragma unroll
+              for (int d = 0; d < 15; ++d)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) asm volatile("" : "+r"(a[d][c]));
+              fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(acc_empty + ab);
+#pragma unroll
+              for (int c = 0; c < 8; ++c) {
+                // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: V_d = S_d + 8 S_(d+8) < 2^29.
+                uint32_t V[8];
+#pragma unroll
+                for (int d = 0; d < 7; ++d) V[d] = a[d][c] + 8u * a[d + 8][c];
+                V[7] = a[7][c];
+                const uint64_t W0 = (uint64_t)V[0] + ((uint64_t)V[1] << 8) + ((uint64_t)V[2] << 16) +
+                                    ((uint64_t)V[3] << 24);  // < 2^54
+                const uint64_t W1 = (uint64_t)V[4] + ((uint64_t)V[5] << 8) + ((uint64_t)V[6] << 16) +
+                                    ((uint64_t)V[7] << 24);  // < 2^54
+                // W0 + 2^32 W1 mod p, with 2^32 W1 = ((W1 << 32) mod 2^61) + (W1 >> 29) mod p.
+                uint64_t x = W0 + ((W1 << 32) & kM61) + (W1 >> 29);  // < 2^62
+                x = (x & kM61) + (x >> 61);
+                if (x >= kM61) x -= kM61;
+                res[c] = f.sub(cv[c], x);
+              }
+            } else {
+              u128 lo[8], hi[8];
+#pragma unroll
+              for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
+#pragma unroll 1
+              for (int d = 0; d < SH::DIAG; ++d) {
+                uint32_t a[8];
+                tmem_ld8(lane_addr + d * NS, a);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                  asm volatile("" : "+r"(a[c]));
+                  if (d < 8)
+                    lo[c] += (u128)a[c] << (8 * d);
+                  else
+                    hi[c] += (u128)a[c] << (8 * (d - 8));
+                }
+              }
+              fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(acc_empty + ab);
+#pragma unroll
+              for (int c = 0; c < 8; ++c) res[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
+            }
+            if (row_ok) {
+#pragma unroll
+              for (int c = 0; c < 8; ++c)
+                if (c0 + c < cend) my[c] = res[c];
+            }
+          }
+          epi_bar();  // results of all rows in shared memory
+          if (ok) {
+            const int64_t gc = (int64_t)jend + (int64_t)s * NS + cc;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int lr = ew * 16 + 2 * i + rr;
+              const int64_t gr = base + lr;
+              if (gr < rend && gc < cend) m[gr * ld + gc] = slot[lr * kCStride + cc];
+            }
+          }
+        }
+      }
+    } else {
+      // Fewer limbs (p < 2^32): NS >= 32 columns per subtile; direct access.
+      for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
+        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+        const int64_t r = (int64_t)rbeg + (int64_t)mt * 128 + row;
+        const bool row_ok = r < rend;
+        for (int s = s0; s < s1; ++s, ++it) {
+          const int ab = it & 1;
+          const uint32_t lane_addr = lane_base + ab * 256;
+          ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
+          if (!ok) break;
+          fence_after();
+          for (int q = 0; q < NS / 16; ++q) {
+            const int64_t c0 = (int64_t)jend + (int64_t)s * NS + q * 16 + half * 8;
+            uint64_t* crow = m + r * ld + c0;
+            uint64_t cv[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
-          }
-          u128 lo[8], hi[8];
+            u128 lo[8], hi[8];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
-          if constexpr (std::is_same<F, FpM61>::value && LIMBS == 8) {
-            // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: fold block d+8 into d.
-#pragma unroll
-            for (int d = 0; d < 15; ++d) {
-              uint32_t a[8];
-              tmem_ld8(lane_addr + d * NS + q * 16, a);
-              tmem_wait_ld();
-              const int sh = d < 8 ? 8 * d : 8 * (d - 8) + 3;
-#pragma unroll
-              for (int c = 0; c < 8; ++c) lo[c] += (u128)a[c] << sh;
-            }
-          } else {
+            for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
 #pragma unroll 1
             for (int d = 0; d < SH::DIAG; ++d) {
               uint32_t a[8];
@@ -403,27 +537,28 @@ __global__ void __launch_bounds__(kThreads, 2)
               tmem_wait_ld();
 #pragma unroll
               for (int c = 0; c < 8; ++c) {
+                asm volatile("" : "+r"(a[c]));
                 if (d < 8)
                   lo[c] += (u128)a[c] << (8 * d);
                 else
                   hi[c] += (u128)a[c] << (8 * (d - 8));
               }
             }
-          }
-          if (q == NS / 16 - 1) {
-            // All accumulator reads done: hand TMEM back to the MMA warp.
-            fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acc_empty);
-          }
-          if (row_ok) {
+            if (q == NS / 16 - 1) {
+              fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(acc_empty + ab);
+            }
+            if (row_ok) {
 #pragma unroll
-            for (int c = 0; c < 8; ++c)
-              if (c0 + c < cend) crow[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
+              for (int c = 0; c < 8; ++c)
+                if (c0 + c < cend) crow[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
+            }
           }
         }
       }
     }
+    cp_async_wait<0>();  // no prefetch may still target this CTA's shared memory
     if (!ok) atomicExch(err, 1);
   }
   fence_before();
@@ -452,7 +587,7 @@ cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, in
   Sched S;
   S.mtiles = mtiles;
   S.nsub = nsub;
-  const int ctas = 2 * num_sms;
+  const int ctas = num_sms;  // one CTA per SM: it owns all 512 TMEM columns
   // Chunk the N subtiles so that there are >= ~2 units per CTA when possible.
   int chunk = nsub;
   while (chunk > 8 && (int64_t)mtiles * ((nsub + chunk - 1) / chunk) < 2 * ctas) chunk = (chunk + 1) / 2;
