@@ -25,9 +25,10 @@
 // limb planes are written to global memory in exactly that layout by the
 // split kernels, so each stage is one contiguous bulk copy.
 //
-// CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
-// the MMAs (one thread), warps 2-9 drain TMEM (warp w reads lanes
-// 32*(w%4)..+32, 8 of every 16 columns). A CTA keeps its 128-row A tile (all limb planes) resident
+// CTA = 18 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
+// the MMAs (one thread), warps 2-17 drain TMEM (warp w reads lanes
+// 32*(w%4)..+32, 4 of every 16 columns). Each CTA takes a contiguous range of
+// the (M tile, N subtile) space; it keeps the 128-row A tile (all limb planes) resident
 // and streams B subtiles through a 6-stage ring; one CTA per SM owns all 512
 // TMEM columns as two accumulator buffers, so the MMAs of subtile s+1 run
 // while the epilogue drains subtile s. Every
@@ -49,10 +50,11 @@ namespace tc {
 constexpr int kK = 64;          // K (panel width) of one update, zero padded
 constexpr int kStages = 6;      // B ring depth
 constexpr int kTileBytes = 8192;  // one 128-row x 64-byte limb plane tile
-constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
+constexpr int kEpiWarps = 16;                // TMEM-draining warps (4 per lane quadrant)
+constexpr int kThreads = 32 * (2 + kEpiWarps);  // producer warp, MMA warp, epilogue warps
 constexpr uint32_t kTmemCols = 512;  // two accumulator buffers of 256 columns
 constexpr int kCDepth = 4;           // staged C tiles (subtiles) in shared memory
-constexpr int kCStride = 17;         // padded row stride (words) of a staged 128 x 16 C tile
+constexpr int kCStride = 18;         // padded row stride (words) of a staged 128 x 16 C tile (16-byte rows)
 constexpr long long kSpinLimit = 4000000000LL;  // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -72,22 +74,25 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait for the phase of `parity` to complete. false = gave up.
+// Bounded wait for the phase of `parity` to complete. false = gave up (about
+// two seconds without completion, or another role reported an error). Each
+// try_wait may suspend the thread until the phase completes (time hint
+// 1 ms), so waiting threads do not take issue slots from working warps.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err) {
   const uint32_t addr = smem_u32(bar);
   const long long t0 = clock64();
-  for (;;) {
+  for (uint32_t k = 0;; ++k) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(addr), "r"(parity)
+        : "r"(addr), "r"(parity), "r"(1000000u)
         : "memory");
     if (done) return true;
     if (clock64() - t0 > kSpinLimit) return false;
-    if (*(volatile const int*)err) return false;
+    if ((k & 15) == 15 && *(volatile const int*)err) return false;
   }
 }
 
@@ -139,6 +144,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "memory");
 }
 
+// 32 lanes x 4 consecutive 32-bit TMEM columns -> 4 registers per thread.
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr)
+               : "memory");
+}
+
 // 32 lanes x 8 consecutive 32-bit TMEM columns -> 8 registers per thread.
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -149,6 +162,9 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -170,8 +186,7 @@ struct Shape {
 };
 
 struct Sched {
-  int mtiles, nsub, chunk, nchunks;
-  __device__ __forceinline__ int units() const { return mtiles * nchunks; }
+  int mtiles, nsub;
 };
 
 // ---------------------------------------------------------------------------
@@ -258,9 +273,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   using SH = Shape<LIMBS>;
   constexpr int NS = SH::NS;
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* sA = smem;                                          // A_BYTES
-  uint8_t* sB = smem + SH::A_BYTES;                            // kStages * 8 KB
-  uint8_t* sZ = sB + kStages * SH::B_BYTES;                    // 4 KB of zeros
+  uint8_t* sA = smem;                        // A_BYTES
+  uint8_t* sB = smem + SH::A_BYTES;          // kStages * 8 KB
+  uint8_t* sZ = sB + kStages * SH::B_BYTES;  // 4 KB of zeros
   uint64_t* bars = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES);
   uint64_t* sC = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024);  // [kCDepth][128][kCStride]
   uint64_t* a_full = bars + 0;
@@ -280,12 +295,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(a_empty, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(acc_full + b, 1);
-      mbar_init(acc_empty + b, 8);
+      mbar_init(acc_empty + b, kEpiWarps);
     }
     mbar_init(mma_done, 1);
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(b_full + s, 1);
-      mbar_init(b_empty + s, 1);
+    for (int st = 0; st < kStages; ++st) {
+      mbar_init(b_full + st, 1);
+      mbar_init(b_empty + st, 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -301,29 +316,34 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   fence_after();
   const uint32_t tmem = tmem_base_sh;
-  const int units = S.units();
+  // This CTA's contiguous range of the (M tile, N subtile) space, row-major:
+  // balanced to one subtile, and an A tile is loaded once per M tile touched.
+  const int64_t total = (int64_t)S.mtiles * S.nsub;
+  const int64_t g0 = total * blockIdx.x / gridDim.x, g1 = total * (blockIdx.x + 1) / gridDim.x;
 
   if (warp == 0) {
     // ---------------- producer: bulk copies -------------------------------
     if (lane == 0) {
-      int it = 0, u_local = 0;
+      int cur = -1, nload = 0, it = 0;
+      int mt = (int)(g0 / S.nsub), sb = (int)(g0 - (int64_t)mt * S.nsub);
       bool ok = true;
-      for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++u_local) {
-        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
-        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
-        if (u_local > 0 && !(ok = mbar_wait(a_empty, (u_local - 1) & 1, err))) break;
-        mbar_arrive_expect_tx(a_full, SH::A_BYTES);
-        bulk_g2s(sA, Aw + (int64_t)mt * SH::A_BYTES, SH::A_BYTES, a_full);
-        for (int s = s0; s < s1; ++s, ++it) {
-          const int st = it % kStages;
-          if (it >= kStages && !(ok = mbar_wait(b_empty + st, ((it / kStages) - 1) & 1, err))) break;
-          mbar_arrive_expect_tx(b_full + st, SH::B_BYTES);
-          bulk_g2s(sB + st * SH::B_BYTES, Bw + (int64_t)s * SH::B_BYTES, SH::B_BYTES, b_full + st);
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
+        if (mt != cur) {
+          if (nload > 0 && !(ok = mbar_wait(a_empty, (nload - 1) & 1, err))) break;
+          mbar_arrive_expect_tx(a_full, SH::A_BYTES);
+          bulk_g2s(sA, Aw + (int64_t)mt * SH::A_BYTES, SH::A_BYTES, a_full);
+          cur = mt;
+          ++nload;
         }
+        const int st = it % kStages;
+        if (it >= kStages && !(ok = mbar_wait(b_empty + st, ((it / kStages) - 1) & 1, err))) break;
+        mbar_arrive_expect_tx(b_full + st, SH::B_BYTES);
+        bulk_g2s(sB + st * SH::B_BYTES, Bw + (int64_t)sb * SH::B_BYTES, SH::B_BYTES, b_full + st);
       }
       if (!ok) {
         atomicExch(err, 1);
         // Let this CTA's own copies land before the CTA can exit.
+        if (nload > 0) mbar_wait(a_full, (nload - 1) & 1, err + 1);
         for (int st = 0; st < kStages; ++st)
           if (it > st) mbar_wait(b_full + st, ((it - 1 - st) / kStages) & 1, err + 1);
       }
@@ -331,36 +351,36 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer ------------------------------------------
     if (lane == 0) {
-      int it = 0, u_local = 0;
+      int cur = -1, nload = 0, it = 0;
       bool ok = true;
       const uint32_t id_full = idesc_i8(LIMBS * NS);
       const uint32_t id_zero = idesc_i8(LIMBS > 1 ? (LIMBS - 1) * NS : 16);
-      for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++u_local) {
-        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
-        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
-        (void)mt;
-        if (!(ok = mbar_wait(a_full, u_local & 1, err))) break;
-        fence_after();
-        for (int s = s0; s < s1; ++s, ++it) {
-          const int st = it % kStages;
-          const int ab = it & 1;  // accumulator buffer
-          if (it >= 2 && !(ok = mbar_wait(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
-          if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+      int mt = (int)(g0 / S.nsub), sb = (int)(g0 - (int64_t)mt * S.nsub);
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
+        if (mt != cur) {
+          if (nload > 0) mma_commit(a_empty);  // the previous A tile is free once these MMAs finish
+          if (!(ok = mbar_wait(a_full, nload & 1, err))) break;
           fence_after();
-          const uint8_t* bt = sB + st * SH::B_BYTES;
-          const uint32_t dacc = tmem + ab * 256;
-          if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
-            mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
-#pragma unroll
-          for (int i = 0; i < LIMBS; ++i)
-#pragma unroll
-            for (int ks = 0; ks < kK / 32; ++ks)
-              mma_i8(dacc + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
-                     id_full, (i > 0 || ks > 0) ? 1u : 0u);
-          mma_commit(b_empty + st);
-          mma_commit(acc_full + ab);
+          cur = mt;
+          ++nload;
         }
-        if (ok) mma_commit(a_empty);
+        const int st = it % kStages;
+        const int ab = it & 1;  // accumulator buffer
+        if (it >= 2 && !(ok = mbar_wait(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
+        if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+        fence_after();
+        const uint8_t* bt = sB + st * SH::B_BYTES;
+        const uint32_t dacc = tmem + ab * 256;
+        if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
+          mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
+#pragma unroll
+        for (int i = 0; i < LIMBS; ++i)
+#pragma unroll
+          for (int ks = 0; ks < kK / 32; ++ks)
+            mma_i8(dacc + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
+                   id_full, (i > 0 || ks > 0) ? 1u : 0u);
+        mma_commit(b_empty + st);
+        mma_commit(acc_full + ab);
       }
       if (!ok) atomicExch(err, 1);
       mma_commit(mma_done);
@@ -369,139 +389,173 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncwarp();
   } else {
     // ---------------- epilogue: TMEM -> exact residue -> C -= T -------------
-    // 8 warps: warp w reads TMEM lanes 32*(w%4)..+32 (its rows) and the
-    // 8-column half (w-2)/4 of every 16-column chunk; the accumulator buffer
-    // is released as soon as its columns are in registers.
+    // kEpiWarps warps: warp w reads TMEM lanes 32*(w%4)..+32 (its rows) and
+    // the 4-column quarter (w-2)/4 of every 16-column chunk; the accumulator
+    // buffer is released as soon as its columns are in registers.
+    const int ew = warp - 2;
     const int quad = warp & 3;
-    const int half = (warp - 2) >> 2;
+    const int qc = ew >> 2;  // column quarter
     const int row = quad * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + half * 8;
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + qc * 4;
     int it = 0;
     bool ok = true;
     if constexpr (LIMBS == 8) {
-      // C goes through shared memory so that global accesses are coalesced:
-      // warp w copies rows 16(w-2)..+16 of the 128 x 16 tile (two 128-byte
-      // rows per instruction) kCDepth - 1 subtiles ahead with cp.async, every
+      // C goes through shared memory so that global accesses are coalesced.
+      // The 4 warps of a TMEM lane quadrant form a group that owns rows
+      // 32*quad..+32 of the 128 x 16 tile: warp (quad, qc) copies rows
+      // 32*quad + 8*qc..+8 kCDepth - 1 subtiles ahead with cp.async, every
       // thread then works on its own row in shared memory, and the results
-      // leave the same way. Named barrier 1 synchronises the 8 epilogue warps.
-      const int ew = warp - 2, rr = lane >> 4, cc = lane & 15;
-      auto epi_bar = []() { asm volatile("bar.sync 1, 256;" ::: "memory"); };
-      int pu = blockIdx.x, ps = 0, ps1 = 0, pcount = 0;
-      int64_t pbase = 0;
-      auto pf_unit = [&]() {
-        if (pu < units) {
-          const int mt = pu / S.nchunks, ch = pu - mt * S.nchunks;
-          ps = ch * S.chunk;
-          ps1 = min(S.nsub, ps + S.chunk);
-          pbase = (int64_t)rbeg + (int64_t)mt * 128;
-        }
-      };
+      // leave the same way. Each group synchronises on its own named barrier
+      // (1 + quad), so the four groups drift and their phases overlap.
+      constexpr int kRowsPerWarp = 8;
+      const int rbase_w = quad * 32 + qc * kRowsPerWarp;
+      const int rr = lane >> 4, cc = lane & 15, rr4 = lane >> 3, cc2 = (lane & 7) * 2;
+      auto epi_bar = [quad]() { asm volatile("bar.sync %0, 128;" ::"r"(1 + quad) : "memory"); };
+      // 16-byte copies when every row start is 16-byte aligned and the
+      // subtile is complete, else 8-byte copies.
+      const bool vec_ld = (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0;
+      int64_t pg = g0;
+      int pmt = (int)(g0 / S.nsub), psb = (int)(g0 - (int64_t)pmt * S.nsub);
+      int pcount = 0;
       auto pf_issue = [&]() {
-        if (pu < units) {
+        if (pg < g1) {
+          const int mt = pmt, sb = psb;
+          const int64_t pbase = (int64_t)rbeg + (int64_t)mt * 128;
           uint64_t* slot = sC + (size_t)(pcount % kCDepth) * 128 * kCStride;
-          const int64_t gc = (int64_t)jend + (int64_t)ps * NS + cc;
+          const int64_t sc0 = (int64_t)jend + (int64_t)sb * NS;
+          if (vec_ld && sc0 + 16 <= cend) {
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const int lr = ew * 16 + 2 * i + rr;
-            const int64_t gr = pbase + lr;
-            if (gr < rend && gc < cend) cp_async8(slot + lr * kCStride + cc, m + gr * ld + gc);
+            for (int i = 0; i < kRowsPerWarp / 4; ++i) {
+              const int lr = rbase_w + 4 * i + rr4;
+              const int64_t gr = pbase + lr;
+              if (gr < rend) cp_async16(slot + lr * kCStride + cc2, m + gr * ld + sc0 + cc2);
+            }
+          } else {
+            const int64_t gc = sc0 + cc;
+#pragma unroll
+            for (int i = 0; i < kRowsPerWarp / 2; ++i) {
+              const int lr = rbase_w + 2 * i + rr;
+              const int64_t gr = pbase + lr;
+              if (gr < rend && gc < cend) cp_async8(slot + lr * kCStride + cc, m + gr * ld + gc);
+            }
           }
-          if (++ps == ps1) {
-            pu += gridDim.x;
-            pf_unit();
+          ++pg;
+          if (++psb == S.nsub) {
+            psb = 0;
+            ++pmt;
           }
         }
         cp_async_commit();
         ++pcount;
       };
-      pf_unit();
       for (int k = 0; k < kCDepth - 1; ++k) pf_issue();
-      for (int u = blockIdx.x; u < units; u += gridDim.x) {
-        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
-        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+      int mt = (int)(g0 / S.nsub), sb = (int)(g0 - (int64_t)mt * S.nsub);
+      for (int64_t g = g0; g < g1; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
         const int64_t base = (int64_t)rbeg + (int64_t)mt * 128;
         const bool row_ok = base + row < rend;
-        for (int s = s0; s < s1; ++s, ++it) {
-          const int ab = it & 1;
-          const uint32_t lane_addr = lane_base + ab * 256;
-          cp_async_wait<kCDepth - 2>();
-          epi_bar();  // this subtile's C is in shared memory; the previous one has been stored
-          pf_issue();
-          uint64_t* slot = sC + (size_t)(it % kCDepth) * 128 * kCStride;
-          uint64_t* my = slot + row * kCStride + half * 8;
-          const int64_t c0 = (int64_t)jend + (int64_t)s * NS + half * 8;
-          uint64_t cv[8];
+        const int ab = it & 1;
+        const uint32_t lane_addr = lane_base + ab * 256;
+        cp_async_wait<kCDepth - 2>();
+        epi_bar();  // this subtile's C is in shared memory; the previous one has been stored
+        pf_issue();
+        uint64_t* slot = sC + (size_t)(it % kCDepth) * 128 * kCStride;
+        uint64_t* my = slot + row * kCStride + qc * 4;
+        const int64_t c0 = (int64_t)jend + (int64_t)sb * NS + qc * 4;
+        uint64_t cv[4];
+        {
+          const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(my);
+          const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(my + 2);
+          cv[0] = v0.x;
+          cv[1] = v0.y;
+          cv[2] = v1.x;
+          cv[3] = v1.y;
+        }
+        if (ok) ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
+        if (ok) {
+          fence_after();
+          uint64_t res[4];
+          if constexpr (std::is_same<F, FpM61>::value) {
+            uint32_t a[15][4];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) cv[c] = my[c];
-          if (ok) ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
-          if (ok) {
-            fence_after();
-            uint64_t res[8];
-            if constexpr (std::is_same<F, FpM61>::value) {
-              uint32_t a[15][8];
+            for (int d = 0; d < 15; ++d) tmem_ld4(lane_addr + d * NS, a[d]);
+            tmem_wait_ld();
 #pragma unroll
-              for (int d = 0; d < 15; ++d) tmem_ld8(lane_addr + d * NS, a[d]);
+            for (int d = 0; d < 15; ++d)
+#pragma unroll
+              for (int c = 0; c < 4; ++c) asm volatile("" : "+r"(a[d][c]));
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty + ab);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: V_d = S_d + 8 S_(d+8) < 2^29.
+              uint32_t V[8];
+#pragma unroll
+              for (int d = 0; d < 7; ++d) V[d] = a[d][c] + 8u * a[d + 8][c];
+              V[7] = a[7][c];
+              // u32 x u32 + u64 multiply-adds (one IMAD.WIDE each).
+              const uint64_t W0 = (uint64_t)V[3] * 16777216u +
+                                  ((uint64_t)V[2] * 65536u + ((uint64_t)V[1] * 256u + (uint64_t)V[0]));
+              const uint64_t W1 = (uint64_t)V[7] * 16777216u +
+                                  ((uint64_t)V[6] * 65536u + ((uint64_t)V[5] * 256u + (uint64_t)V[4]));
+              // W0 + 2^32 W1 mod p, with 2^32 W1 = ((W1 mod 2^29) << 32) + (W1 >> 29) mod p.
+              uint64_t x = W0 + ((uint64_t)((uint32_t)W1 & 0x1FFFFFFFu) << 32) + (W1 >> 29);  // < 2^62
+              x = (x & kM61) + (x >> 61);
+              x = x >= kM61 ? x - kM61 : x;
+              res[c] = cv[c] >= x ? cv[c] - x : cv[c] + kM61 - x;
+            }
+          } else {
+            u128 lo[4], hi[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) lo[c] = hi[c] = 0;
+#pragma unroll 1
+            for (int d = 0; d < SH::DIAG; ++d) {
+              uint32_t a[4];
+              tmem_ld4(lane_addr + d * NS, a);
               tmem_wait_ld();
 #pragma unroll
-              for (int d = 0; d < 15; ++d)
-#pragma unroll
-                for (int c = 0; c < 8; ++c) asm volatile("" : "+r"(a[d][c]));
-              fence_before();
-              __syncwarp();
-              if (lane == 0) mbar_arrive(acc_empty + ab);
-#pragma unroll
-              for (int c = 0; c < 8; ++c) {
-                // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: V_d = S_d + 8 S_(d+8) < 2^29.
-                uint32_t V[8];
-#pragma unroll
-                for (int d = 0; d < 7; ++d) V[d] = a[d][c] + 8u * a[d + 8][c];
-                V[7] = a[7][c];
-                const uint64_t W0 = (uint64_t)V[0] + ((uint64_t)V[1] << 8) + ((uint64_t)V[2] << 16) +
-                                    ((uint64_t)V[3] << 24);  // < 2^54
-                const uint64_t W1 = (uint64_t)V[4] + ((uint64_t)V[5] << 8) + ((uint64_t)V[6] << 16) +
-                                    ((uint64_t)V[7] << 24);  // < 2^54
-                // W0 + 2^32 W1 mod p, with 2^32 W1 = ((W1 << 32) mod 2^61) + (W1 >> 29) mod p.
-                uint64_t x = W0 + ((W1 << 32) & kM61) + (W1 >> 29);  // < 2^62
-                x = (x & kM61) + (x >> 61);
-                if (x >= kM61) x -= kM61;
-                res[c] = f.sub(cv[c], x);
+              for (int c = 0; c < 4; ++c) {
+                asm volatile("" : "+r"(a[c]));
+                if (d < 8)
+                  lo[c] += (u128)a[c] << (8 * d);
+                else
+                  hi[c] += (u128)a[c] << (8 * (d - 8));
               }
-            } else {
-              u128 lo[8], hi[8];
-#pragma unroll
-              for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
-#pragma unroll 1
-              for (int d = 0; d < SH::DIAG; ++d) {
-                uint32_t a[8];
-                tmem_ld8(lane_addr + d * NS, a);
-                tmem_wait_ld();
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                  asm volatile("" : "+r"(a[c]));
-                  if (d < 8)
-                    lo[c] += (u128)a[c] << (8 * d);
-                  else
-                    hi[c] += (u128)a[c] << (8 * (d - 8));
-                }
-              }
-              fence_before();
-              __syncwarp();
-              if (lane == 0) mbar_arrive(acc_empty + ab);
-#pragma unroll
-              for (int c = 0; c < 8; ++c) res[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
             }
-            if (row_ok) {
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty + ab);
 #pragma unroll
-              for (int c = 0; c < 8; ++c)
+            for (int c = 0; c < 4; ++c) res[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
+          }
+          if (row_ok) {
+            if (c0 + 4 <= cend) {
+              *reinterpret_cast<ulonglong2*>(my) = make_ulonglong2(res[0], res[1]);
+              *reinterpret_cast<ulonglong2*>(my + 2) = make_ulonglong2(res[2], res[3]);
+            } else {
+#pragma unroll
+              for (int c = 0; c < 4; ++c)
                 if (c0 + c < cend) my[c] = res[c];
             }
           }
-          epi_bar();  // results of all rows in shared memory
-          if (ok) {
-            const int64_t gc = (int64_t)jend + (int64_t)s * NS + cc;
+        }
+        epi_bar();  // results of all rows in shared memory
+        if (ok) {
+          const int64_t sc0 = (int64_t)jend + (int64_t)sb * NS;
+          if (vec_ld && sc0 + 16 <= cend) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-              const int lr = ew * 16 + 2 * i + rr;
+            for (int i = 0; i < kRowsPerWarp / 4; ++i) {
+              const int lr = rbase_w + 4 * i + rr4;
+              const int64_t gr = base + lr;
+              if (gr < rend)
+                *reinterpret_cast<ulonglong2*>(m + gr * ld + sc0 + cc2) =
+                    *reinterpret_cast<const ulonglong2*>(slot + lr * kCStride + cc2);
+            }
+          } else {
+            const int64_t gc = sc0 + cc;
+#pragma unroll
+            for (int i = 0; i < kRowsPerWarp / 2; ++i) {
+              const int lr = rbase_w + 2 * i + rr;
               const int64_t gr = base + lr;
               if (gr < rend && gc < cend) m[gr * ld + gc] = slot[lr * kCStride + cc];
             }
@@ -510,50 +564,47 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     } else {
       // Fewer limbs (p < 2^32): NS >= 32 columns per subtile; direct access.
-      for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
-        const int mt = u / S.nchunks, ch = u - mt * S.nchunks;
-        const int s0 = ch * S.chunk, s1 = min(S.nsub, s0 + S.chunk);
+      int mt = (int)(g0 / S.nsub), sb = (int)(g0 - (int64_t)mt * S.nsub);
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
         const int64_t r = (int64_t)rbeg + (int64_t)mt * 128 + row;
         const bool row_ok = r < rend;
-        for (int s = s0; s < s1; ++s, ++it) {
-          const int ab = it & 1;
-          const uint32_t lane_addr = lane_base + ab * 256;
-          ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
-          if (!ok) break;
-          fence_after();
-          for (int q = 0; q < NS / 16; ++q) {
-            const int64_t c0 = (int64_t)jend + (int64_t)s * NS + q * 16 + half * 8;
-            uint64_t* crow = m + r * ld + c0;
-            uint64_t cv[8];
+        const int ab = it & 1;
+        const uint32_t lane_addr = lane_base + ab * 256;
+        ok = __all_sync(0xffffffffu, mbar_wait(acc_full + ab, (it >> 1) & 1, err));
+        if (!ok) break;
+        fence_after();
+        for (int q = 0; q < NS / 16; ++q) {
+          const int64_t c0 = (int64_t)jend + (int64_t)sb * NS + q * 16 + qc * 4;
+          uint64_t* crow = m + r * ld + c0;
+          uint64_t cv[4];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
-            u128 lo[8], hi[8];
+          for (int c = 0; c < 4; ++c) cv[c] = (row_ok && c0 + c < cend) ? crow[c] : 0;
+          u128 lo[4], hi[4];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) lo[c] = hi[c] = 0;
+          for (int c = 0; c < 4; ++c) lo[c] = hi[c] = 0;
 #pragma unroll 1
-            for (int d = 0; d < SH::DIAG; ++d) {
-              uint32_t a[8];
-              tmem_ld8(lane_addr + d * NS + q * 16, a);
-              tmem_wait_ld();
+          for (int d = 0; d < SH::DIAG; ++d) {
+            uint32_t a[4];
+            tmem_ld4(lane_addr + d * NS + q * 16, a);
+            tmem_wait_ld();
 #pragma unroll
-              for (int c = 0; c < 8; ++c) {
-                asm volatile("" : "+r"(a[c]));
-                if (d < 8)
-                  lo[c] += (u128)a[c] << (8 * d);
-                else
-                  hi[c] += (u128)a[c] << (8 * (d - 8));
-              }
+            for (int c = 0; c < 4; ++c) {
+              asm volatile("" : "+r"(a[c]));
+              if (d < 8)
+                lo[c] += (u128)a[c] << (8 * d);
+              else
+                hi[c] += (u128)a[c] << (8 * (d - 8));
             }
-            if (q == NS / 16 - 1) {
-              fence_before();
-              __syncwarp();
-              if (lane == 0) mbar_arrive(acc_empty + ab);
-            }
-            if (row_ok) {
+          }
+          if (q == NS / 16 - 1) {
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty + ab);
+          }
+          if (row_ok) {
 #pragma unroll
-              for (int c = 0; c < 8; ++c)
-                if (c0 + c < cend) crow[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
-            }
+            for (int c = 0; c < 4; ++c)
+              if (c0 + c < cend) crow[c] = f.sub(cv[c], finish(f, lo[c], hi[c], r64));
           }
         }
       }
@@ -587,14 +638,8 @@ cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, in
   Sched S;
   S.mtiles = mtiles;
   S.nsub = nsub;
-  const int ctas = num_sms;  // one CTA per SM: it owns all 512 TMEM columns
-  // Chunk the N subtiles so that there are >= ~2 units per CTA when possible.
-  int chunk = nsub;
-  while (chunk > 8 && (int64_t)mtiles * ((nsub + chunk - 1) / chunk) < 2 * ctas) chunk = (chunk + 1) / 2;
-  S.chunk = chunk;
-  S.nchunks = (nsub + chunk - 1) / chunk;
-  const int units = S.mtiles * S.nchunks;
-  const int grid = units < ctas ? units : ctas;
+  const int64_t total = (int64_t)mtiles * nsub;
+  const int grid = total < num_sms ? (int)total : num_sms;  // one CTA per SM: it owns all 512 TMEM columns
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
