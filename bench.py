@@ -169,6 +169,137 @@ def cpu_rank_sample(threads=0, target_s=12.0):
     return {"value": w / dt, "seconds": dt, "n": n, "rank": r, "work": w}
 
 
+def splitmix64(seed):
+    """SplitMix64 outputs (the workload generators' seeding convention)."""
+    z = seed & 0xFFFFFFFFFFFFFFFF
+    while True:
+        z = (z + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        w = z
+        w = ((w ^ (w >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        w = ((w ^ (w >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        yield w ^ (w >> 31)
+
+
+BM_PRIMES = [65521, (1 << 31) - 1, M61]
+
+
+def bm_batch_jobs(count=65536, seed=31, nmin=256, nmax=8192):
+    """The batched Berlekamp-Massey workload: `count` sequences, lengths
+    uniform in [nmin, nmax], primes equally from BM_PRIMES, odd-indexed jobs
+    planted order-L recurrences with L uniform in [16, n/4], even-indexed jobs
+    iid uniform residues. Per job (prime index, n, L, seed) come from
+    SplitMix64(seed); a planted job's stream is SplitMix64(its seed) through
+    the planted generator, the iid jobs of one prime are consecutive slices of
+    one uniform stream per prime."""
+    g = splitmix64(seed)
+    jobs = []
+    for i in range(count):
+        pi = next(g) % 3
+        n = nmin + next(g) % (nmax - nmin + 1)
+        planted = i % 2 == 1
+        L = 16 + next(g) % (n // 4 - 16 + 1)
+        jobs.append((pi, n, planted, L if planted else None, next(g)))
+    iid_seeds = [next(g) for _ in range(3)]
+    return jobs, iid_seeds
+
+
+def bm_batch_build(torch, modlin, jobs, iid_seeds):
+    """Device buffers of the batch: one arena, planted jobs by one launch of
+    the planted generator, iid jobs by one uniform stream per prime."""
+    total = sum(j[1] for j in jobs)
+    arena = torch.empty(total, dtype=torch.int64, device="cuda")
+    base = arena.data_ptr()
+    ptrs, off = [], 0
+    for j in jobs:
+        ptrs.append(base + 8 * off)
+        off += j[1]
+    pl = [i for i, j in enumerate(jobs) if j[2]]
+    modlin.gen.planted_batch_device([BM_PRIMES[jobs[i][0]] for i in pl], [jobs[i][3] for i in pl],
+                                    [jobs[i][4] for i in pl], [ptrs[i] for i in pl], [jobs[i][1] for i in pl])
+    for pi in range(3):
+        ids = [i for i, j in enumerate(jobs) if not j[2] and j[0] == pi]
+        cnt = sum(jobs[i][1] for i in ids)
+        if not cnt:
+            continue
+        tmp = torch.empty(cnt, dtype=torch.int64, device="cuda")
+        modlin.gen.uniform_device(BM_PRIMES[pi], iid_seeds[pi], tmp.data_ptr(), cnt)
+        o = 0
+        for i in ids:
+            n = jobs[i][1]
+            arena[(ptrs[i] - base) // 8:(ptrs[i] - base) // 8 + n].copy_(tmp[o:o + n])
+            o += n
+        del tmp
+    torch.cuda.synchronize()
+    return arena, ptrs
+
+
+def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, batch_count=65536,
+               plain_sample=512):
+    """Berlekamp-Massey throughput (steps = sequence elements processed):
+    the two long sequences on the cooperative grid kernel, the batch in one
+    persistent launch, and the plain one-sequence-per-launch form on a
+    sample of the same batch."""
+    from modlin import fp as mfp
+    res = {}
+    for name, planted, seed in (("long_planted", True, 21), ("long_iid", False, 22)):
+        t = torch.empty(long_n, dtype=torch.int64, device="cuda")
+        if planted:
+            modlin.gen.planted_device(M61, long_L, seed, t.data_ptr(), long_n)
+        else:
+            modlin.gen.uniform_device(M61, seed, t.data_ptr(), long_n)
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel="grid")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel="grid")
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[name] = {"n": long_n, "lc": lc, "expected": long_L if planted else "about n/2", "ms": ms,
+                     "steps_per_s": long_n / (ms * 1e-3)}
+        if planted:
+            assert lc == long_L, (lc, long_L)
+        del t
+    jobs, iid_seeds = bm_batch_jobs(batch_count)
+    arena, ptrs = bm_batch_build(torch, modlin, jobs, iid_seeds)
+    ps = [BM_PRIMES[j[0]] for j in jobs]
+    ns = [j[1] for j in jobs]
+    total = sum(ns)
+    for _ in range(warmup):
+        lcs = mfp.lc_batch_device(ps, ptrs, ns)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        lcs = mfp.lc_batch_device(ps, ptrs, ns)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    bad = [i for i, j in enumerate(jobs) if j[2] and lcs[i] != j[3]]
+    assert not bad, bad[:5]
+    iid_dev = max(abs(lcs[i] - (j[1] + 1) // 2) for i, j in enumerate(jobs) if not j[2])
+    batch = {"sequences": len(jobs), "total_steps": total, "ms": ms, "steps_per_s": total / (ms * 1e-3),
+             "planted_exact": True, "iid_max_dev_from_half": iid_dev}
+    # Plain form: one sequence per launch, each call waits for its result.
+    idx = list(range(0, len(jobs), max(1, len(jobs) // plain_sample)))[:plain_sample]
+    sub = sum(ns[i] for i in idx)
+    mfp.linear_complexity_device(ps[idx[0]], ptrs[idx[0]], ns[idx[0]], kernel="block")
+    torch.cuda.synchronize()
+    e0.record()
+    for i in idx:
+        assert mfp.linear_complexity_device(ps[i], ptrs[i], ns[i], kernel="block") == lcs[i]
+    e1.record()
+    torch.cuda.synchronize()
+    pms = e0.elapsed_time(e1)
+    batch["plain_one_per_launch"] = {"sequences": len(idx), "steps": sub, "ms": pms,
+                                     "steps_per_s": sub / (pms * 1e-3)}
+    batch["speedup_vs_plain"] = batch["steps_per_s"] / batch["plain_one_per_launch"]["steps_per_s"]
+    res["batch"] = batch
+    del arena
+    return res
+
+
 def host_cores():
     try:
         import oracle
@@ -227,6 +358,8 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--workload", default="rank", choices=["rank", "bm"],
+                    help="rank: the 16384^2 rank (default line); bm: only the Berlekamp-Massey measurements")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -245,6 +378,12 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     import modlin
     from modlin import fp as mfp
+
+    if args.workload == "bm":
+        res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
+        if rank == 0:
+            print(json.dumps({"workload": "berlekamp-massey", **res}), flush=True)
+        return
 
     n = args.n
     kernel = args.kernel
@@ -315,6 +454,8 @@ def main():
             torch.cuda.synchronize()
             extras["plain_modmac_per_s"] = W / (e0.elapsed_time(e1) * 1e-3)
             extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
+        # Berlekamp-Massey: the long sequences and the 65536-sequence batch.
+        extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128)
 
     # End to end through the public C ABI with host buffers: pinned host
     # matrix -> modlin_rank (H2D copy + rank + D2H of the result) each step.

@@ -189,6 +189,14 @@ int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t *d_out, size_t
  * s_0..s_{L-1} uniform residues from SplitMix64(seed);
  * s[i] = sum_{j=1..L} a_j s[i-j] mod p. */
 int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t *out, size_t count);
+/* Same streams as modlin_gen_planted, produced on the device: the 2L seeded
+ * draws (coefficients, initial state) on the host, the recurrence extended
+ * by one CTA per sequence. Bit-identical to the host generator. */
+int modlin_gen_planted_device(uint64_t p, size_t L, uint64_t seed, uint64_t *d_out, size_t count, void *stream);
+/* A batch of planted sequences, job i: prime p[i], order L[i], seed seed[i],
+ * count[i] outputs at device pointer d_out[i]; all in one launch. */
+int modlin_gen_planted_batch_device(const uint64_t *p, const size_t *L, const uint64_t *seed,
+                                    uint64_t *const *d_out, const size_t *count, size_t njobs, void *stream);
 /* Field::reduce on the device, in place (src/main.rs:94-104 fill). */
 int modlin_reduce_device(uint64_t p, uint64_t *d_x, size_t count, void *stream);
 

@@ -58,6 +58,7 @@ struct Ctx {
   int2* h_moves = nullptr;
   // linear-complexity workspaces
   DevBuf seq, bmws, bmout, bmsync, bmjobs, bmnext;
+  DevBuf gena, genjobs;  // planted-generator coefficients and jobs
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
 };
@@ -590,13 +591,13 @@ int modlin_gen_uniform(uint64_t p, uint64_t seed, uint64_t* out, size_t count) {
   return MODLIN_OK;
 }
 
-int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t* out, size_t count) {
-  FieldParams fp;
-  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
-  if (!out && count) return MODLIN_EINVAL_ARG;
-  std::vector<uint64_t> a(L + 1), init(L);
-  std::vector<uint64_t> draws(1);
-  // Coefficients a_1..a_L, a_L redrawn while 0, then initial values.
+}  // extern "C"
+
+// Planted recurrence parameters from SplitMix64(seed): a_1..a_L (a_L redrawn
+// while 0), then the initial values s_0..s_{L-1}, all uniform residues.
+static void draw_planted(uint64_t p, size_t L, uint64_t seed, std::vector<uint64_t>& a, std::vector<uint64_t>& init) {
+  a.assign(L + 1, 0);
+  init.assign(L, 0);
   uint64_t z = seed;
   const int bits = 64 - __builtin_clzll(p - 1);
   auto uni = [&]() {
@@ -613,6 +614,16 @@ int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t* out, size_
   for (size_t j = 1; j <= L; ++j) a[j] = uni();
   while (L > 0 && a[L] == 0) a[L] = uni();
   for (size_t i = 0; i < L; ++i) init[i] = uni();
+}
+
+extern "C" {
+
+int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t* out, size_t count) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!out && count) return MODLIN_EINVAL_ARG;
+  std::vector<uint64_t> a, init;
+  draw_planted(p, L, seed, a, init);
   const FpBarrett f(fp);
   const uint64_t sb = fp.safe_batch;
   for (size_t i = 0; i < count; ++i) {
@@ -633,6 +644,62 @@ int modlin_gen_planted(uint64_t p, size_t L, uint64_t seed, uint64_t* out, size_
     out[i] = f.add(tot, f.reduce(acc));
   }
   return MODLIN_OK;
+}
+
+int modlin_gen_planted_batch_device(const uint64_t* p, const size_t* L, const uint64_t* seed, uint64_t* const* d_out,
+                                    const size_t* count, size_t njobs, void* stream) {
+  if (njobs && (!p || !L || !seed || !d_out || !count)) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  size_t total_a = 0;
+  for (size_t i = 0; i < njobs; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    if (!d_out[i] && count[i]) return MODLIN_EINVAL_ARG;
+    total_a += L[i];
+  }
+  std::vector<uint64_t> coeffs;
+  coeffs.reserve(total_a);
+  std::vector<PlantJob> jobs;
+  std::vector<uint64_t> a, init;
+  CK(C->gena.ensure(std::max<size_t>(total_a, 1) * 8));
+  size_t off = 0;
+  for (size_t i = 0; i < njobs; ++i) {
+    draw_planted(p[i], L[i], seed[i], a, init);
+    coeffs.insert(coeffs.end(), a.begin() + 1, a.end());
+    const size_t ncopy = std::min(L[i], count[i]);
+    if (ncopy) CK(cudaMemcpyAsync(d_out[i], init.data(), ncopy * 8, cudaMemcpyHostToDevice, st));
+    // cudaMemcpyAsync from pageable memory returns after staging the data,
+    // so `init` may be reused for the next job.
+    FieldParams fp;
+    make_field_params(p[i], &fp);
+    if (count[i] > L[i])
+      jobs.push_back(PlantJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, C->gena.as<uint64_t>() + off, d_out[i],
+                              (int64_t)L[i], (int64_t)count[i]});
+    off += L[i];
+  }
+  if (total_a) CK(cudaMemcpyAsync(C->gena.p, coeffs.data(), total_a * 8, cudaMemcpyHostToDevice, st));
+  if (!jobs.empty()) {
+    CK(C->genjobs.ensure(jobs.size() * sizeof(PlantJob)));
+    CK(C->bmnext.ensure(sizeof(unsigned long long)));
+    CK(cudaMemcpyAsync(C->genjobs.p, jobs.data(), jobs.size() * sizeof(PlantJob), cudaMemcpyHostToDevice, st));
+    size_t maxL = 0;
+    for (auto& j : jobs) maxL = std::max<size_t>(maxL, (size_t)j.L);
+    const int threads = maxL >= 8192 ? 1024 : (maxL >= 1024 ? 512 : 128);
+    int blocks = C->num_sms * (2048 / threads);
+    if ((size_t)blocks > jobs.size()) blocks = (int)jobs.size();
+    CK(plant_device(C->genjobs.as<PlantJob>(), (int64_t)jobs.size(), C->bmnext.as<unsigned long long>(), blocks,
+                    threads, st));
+    g_launches += 2;
+  }
+  return cuda_rc(cudaStreamSynchronize(st));
+}
+
+int modlin_gen_planted_device(uint64_t p, size_t L, uint64_t seed, uint64_t* d_out, size_t count, void* stream) {
+  return modlin_gen_planted_batch_device(&p, &L, &seed, &d_out, &count, 1, stream);
 }
 
 int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t* d_out, size_t count, void* stream) {

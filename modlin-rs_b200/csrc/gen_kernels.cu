@@ -174,3 +174,71 @@ cudaError_t reduce_device(const FieldParams& fp, uint64_t* d_x, uint64_t count, 
 }
 
 }  // namespace modlin
+
+namespace modlin {
+
+// ---------------------------------------------------------------------------
+// Planted recurrences on the device: each job extends s[0..L) to s[0..n) by
+// s[i] = sum_{j=1..L} a_j s[i-j] mod p (coefficients a[0..L) = a_1..a_L).
+// One CTA per job (persistent over a job counter); every output is a
+// CTA-wide dot product with u128 lazy accumulation, reduced mod p. Exact,
+// so the stream equals the host generator's bit for bit.
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ void plant_extend(const F& f, const uint64_t* __restrict__ a, uint64_t* s, int64_t L, int64_t n,
+                             uint64_t (*ws)[32]) {
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
+  const uint64_t sb = f.safe_batch();
+  for (int64_t i = L; i < n; ++i) {
+    u128 acc = 0;
+    uint64_t tot = 0, cnt = 0;
+    for (int64_t j = tid; j < L; j += T) {
+      acc += (u128)a[j] * s[i - 1 - j];
+      if (++cnt == sb) {
+        tot = f.add(tot, f.reduce(acc));
+        acc = 0;
+        cnt = 0;
+      }
+    }
+    uint64_t part = f.add(tot, f.reduce(acc));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) part = f.add(part, __shfl_down_sync(0xffffffffu, part, off));
+    if (lane == 0) ws[i & 1][warp] = part;
+    __syncthreads();
+    if (tid == 0) {
+      uint64_t v = 0;
+      for (int w = 0; w < nw; ++w) v = f.add(v, ws[i & 1][w]);
+      s[i] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void plant_kernel(const PlantJob* __restrict__ jobs, int64_t count, unsigned long long* next) {
+  __shared__ uint64_t ws[2][32];
+  __shared__ long long q;
+  for (;;) {
+    if (threadIdx.x == 0) q = (long long)atomicAdd(next, 1ULL);
+    __syncthreads();
+    const long long k = q;
+    __syncthreads();
+    if (k >= count) break;
+    const PlantJob J = jobs[k];
+    const FieldParams fp{J.p, J.mu_lo, J.mu_hi, J.safe_batch};
+    if (J.p == kM61)
+      plant_extend(FpM61(fp), J.a, J.s, J.L, J.n, ws);
+    else
+      plant_extend(FpBarrett(fp), J.a, J.s, J.L, J.n, ws);
+    __syncthreads();
+  }
+}
+
+cudaError_t plant_device(const PlantJob* d_jobs, int64_t count, unsigned long long* d_next, int blocks, int threads,
+                         cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  plant_kernel<<<blocks, threads, 0, st>>>(d_jobs, count, d_next);
+  return cudaGetLastError();
+}
+
+}  // namespace modlin

@@ -12,4 +12,15 @@ cudaError_t gen_uniform_device(uint64_t p, uint64_t seed, uint64_t* d_out, uint6
                                uint64_t* launches);
 cudaError_t reduce_device(const FieldParams& fp, uint64_t* d_x, uint64_t count, cudaStream_t st);
 
+// One planted-recurrence extension job (device pointers): s[0..L) given,
+// s[L..n) produced; a[0..L) = a_1..a_L.
+struct PlantJob {
+  uint64_t p, mu_lo, mu_hi, safe_batch;
+  const uint64_t* a;
+  uint64_t* s;
+  int64_t L, n;
+};
+cudaError_t plant_device(const PlantJob* d_jobs, int64_t count, unsigned long long* d_next, int blocks, int threads,
+                         cudaStream_t st);
+
 }  // namespace modlin

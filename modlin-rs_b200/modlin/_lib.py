@@ -89,6 +89,8 @@ def lib():
     _proto(L, "modlin_gen_uniform", ci, [u64, u64, u64p, szt])
     _proto(L, "modlin_gen_uniform_device", ci, [u64, u64, vp, szt, vp])
     _proto(L, "modlin_gen_planted", ci, [u64, szt, u64, u64p, szt])
+    _proto(L, "modlin_gen_planted_device", ci, [u64, szt, u64, vp, szt, vp])
+    _proto(L, "modlin_gen_planted_batch_device", ci, [u64p, sztp, u64p, ctypes.POINTER(vp), sztp, szt, vp])
     _proto(L, "modlin_reduce_device", ci, [u64, vp, szt, vp])
     _proto(L, "modlin_kernel_launches", u64, [])
     _proto(L, "modlin_last_trailing_ms", ctypes.c_double, [])
@@ -111,5 +113,6 @@ EXPORTED = [
     "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue", "modlin_pretty_p_value",
     "modlin_prng_new", "modlin_prng_name", "modlin_prng_fill", "modlin_prng_free",
     "modlin_gen_uniform", "modlin_gen_uniform_device", "modlin_gen_planted", "modlin_reduce_device",
+    "modlin_gen_planted_device", "modlin_gen_planted_batch_device",
     "modlin_kernel_launches", "modlin_last_trailing_ms",
 ]
