@@ -145,6 +145,11 @@ typedef struct {
 /* Ranks of `count` matrices of any sides and primes in one persistent
  * launch (matrices are copied; the inputs are not modified). */
 int modlin_rank_batch(const modlin_job *jobs, size_t count, size_t *ranks_out);
+/* Device-resident batch: d_m[i] is an n[i] x n[i] row-major matrix mod p[i]
+ * in device memory, clobbered like modlin_rank_device. Sides up to 8192 go
+ * into one persistent launch; larger ones run one after another. */
+int modlin_rank_batch_device(const uint64_t *p, uint64_t *const *d_m, const size_t *n, size_t count,
+                             size_t *ranks_out, void *stream);
 /* Linear complexities of `count` sequences in one persistent launch. */
 int modlin_lc_batch(const modlin_job *jobs, size_t count, size_t *lcs_out);
 

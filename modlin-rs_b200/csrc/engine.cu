@@ -16,6 +16,7 @@
 #include "bm_kernels.cuh"
 #include "field.cuh"
 #include "gen_kernels.cuh"
+#include "rank_batch.cuh"
 #include "rank_kernels.cuh"
 #include "rank_tc.cuh"
 
@@ -59,6 +60,7 @@ struct Ctx {
   // linear-complexity workspaces
   DevBuf seq, bmws, bmout, bmsync, bmjobs, bmnext;
   DevBuf gena, genjobs;  // planted-generator coefficients and jobs
+  DevBuf batchm, rbjobs, rbout;  // batched rank: matrix arena, jobs, ranks
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
 };
@@ -336,6 +338,58 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
   return MODLIN_OK;
 }
 
+// Batched rank: jobs up to kRankBatchMaxN go into one persistent launch
+// (largest first), larger ones through the single-matrix engine afterwards.
+static int rank_batch_locked(Ctx* C, const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
+                             size_t* ranks_out, cudaStream_t st, std::unique_lock<std::mutex>& g) {
+  if (count == 0) return MODLIN_OK;
+  std::vector<RankJob> jobs;
+  std::vector<size_t> big;
+  int64_t maxn = 0;
+  for (size_t i = 0; i < count; ++i) {
+    if (n[i] == 0) {
+      ranks_out[i] = 0;
+      continue;
+    }
+    if ((int64_t)n[i] > kRankBatchMaxN) {
+      big.push_back(i);
+      continue;
+    }
+    FieldParams fp;
+    make_field_params(p[i], &fp);
+    jobs.push_back(RankJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_m[i], (int64_t)n[i], (int64_t)i});
+    maxn = std::max<int64_t>(maxn, (int64_t)n[i]);
+  }
+  if (!jobs.empty()) {
+    // Largest first (work ~ n^3): the persistent CTAs then finish together.
+    std::stable_sort(jobs.begin(), jobs.end(), [](const RankJob& a, const RankJob& b) { return a.n > b.n; });
+    CK(C->rbjobs.ensure(sizeof(RankJob) * jobs.size()));
+    CK(C->bmnext.ensure(sizeof(unsigned long long)));
+    CK(C->rbout.ensure(sizeof(int64_t) * count));
+    CK(cudaMemcpyAsync(C->rbjobs.p, jobs.data(), sizeof(RankJob) * jobs.size(), cudaMemcpyHostToDevice, st));
+    int per_sm = rank_batch_blocks_per_sm(maxn);
+    if (per_sm < 1) return MODLIN_ECUDA;
+    int blocks = C->num_sms * per_sm;
+    if ((size_t)blocks > jobs.size()) blocks = (int)jobs.size();
+    CK(launch_rank_batch(C->rbjobs.as<RankJob>(), (int64_t)jobs.size(), C->bmnext.as<unsigned long long>(), maxn,
+                         blocks, C->rbout.as<int64_t>(), st));
+    g_launches += 2;
+    std::vector<int64_t> out(count);
+    CK(cudaMemcpyAsync(out.data(), C->rbout.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (const RankJob& j : jobs) ranks_out[j.slot] = (size_t)out[j.slot];
+  }
+  if (!big.empty()) {
+    g.unlock();
+    for (size_t i : big) {
+      const int rc2 = modlin_rank_device(p[i], d_m[i], n[i], nullptr, &ranks_out[i], nullptr, st);
+      if (rc2) return rc2;
+    }
+    g.lock();
+  }
+  return MODLIN_OK;
+}
+
 static int lc_batch_locked(Ctx* C, const uint64_t* p, const uint64_t* const* d_data, const size_t* n,
                            size_t count, size_t* lcs_out, cudaStream_t st) {
   if (count == 0) return MODLIN_OK;
@@ -561,17 +615,50 @@ int modlin_lc_batch(const modlin_job* jobs, size_t count, size_t* lcs_out) {
   return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, lcs_out, C->stream);
 }
 
+int modlin_rank_batch_device(const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
+                             size_t* ranks_out, void* stream) {
+  if (count && (!p || !d_m || !n || !ranks_out)) return MODLIN_EINVAL_ARG;
+  for (size_t i = 0; i < count; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    if (n[i] && !d_m[i]) return MODLIN_EINVAL_ARG;
+    if (n[i] > (size_t)INT32_MAX / 2) return MODLIN_EINVAL_N;
+  }
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::unique_lock<std::mutex> g(C->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  return rank_batch_locked(C, p, d_m, n, count, ranks_out, st, g);
+}
+
 int modlin_rank_batch(const modlin_job* jobs, size_t count, size_t* ranks_out) {
   if (count && (!jobs || !ranks_out)) return MODLIN_EINVAL_ARG;
-  // One job after another through the single-matrix engine (the batched
-  // persistent kernel handles this in rank_batch.cu when available).
+  size_t total = 0;
   for (size_t i = 0; i < count; ++i) {
-    std::vector<uint64_t> tmp(jobs[i].data, jobs[i].data + jobs[i].n * jobs[i].n);
-    const int rc = modlin_rank_ex(jobs[i].p, tmp.data(), jobs[i].n, nullptr, &ranks_out[i], nullptr, nullptr,
-                                  nullptr);
-    if (rc) return rc;
+    if (!jobs[i].data && jobs[i].n) return MODLIN_EINVAL_ARG;
+    if (jobs[i].n > (size_t)INT32_MAX / 2) return MODLIN_EINVAL_N;
+    total += jobs[i].n * jobs[i].n;
   }
-  return MODLIN_OK;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::unique_lock<std::mutex> g(C->mu);
+  // All matrices copied into one device arena (the inputs stay untouched).
+  CK(C->batchm.ensure(std::max<size_t>(total, 1) * 8));
+  std::vector<uint64_t*> ptrs(count);
+  std::vector<uint64_t> ps(count);
+  std::vector<size_t> ns(count);
+  size_t off = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const size_t nn = jobs[i].n * jobs[i].n;
+    ptrs[i] = C->batchm.as<uint64_t>() + off;
+    if (nn) CK(cudaMemcpyAsync(ptrs[i], jobs[i].data, nn * 8, cudaMemcpyHostToDevice, C->stream));
+    ps[i] = jobs[i].p;
+    ns[i] = jobs[i].n;
+    off += nn;
+  }
+  return rank_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, ranks_out, C->stream, g);
 }
 
 int modlin_gen_uniform(uint64_t p, uint64_t seed, uint64_t* out, size_t count) {

@@ -3,12 +3,13 @@
 // The contract is the reference's `Field` (src/fp.rs:34-114): canonical
 // residues in [0, p), Barrett reciprocal mu = floor((2^128 - 1) / p) and exact
 // reduction of any 128-bit value, add/sub/mul on canonical inputs, Fermat
-// inverse. Two policies implement it:
+// inverse. Three policies implement it:
 //   * FpBarrett — any p in [2, 2^63): the reference's Barrett reduction
 //     (src/fp.rs:71-79) on 64-bit integer pipes;
 //   * FpM61 — p = 2^61 - 1 (MIXMAX's modulus and every large benchmark
-//     workload): shift-and-add reduction, since 2^61 = 1 mod p.
-// Both return the exact residue, so every kernel built on them is bit-exact.
+//     workload): shift-and-add reduction, since 2^61 = 1 mod p;
+//   * FpSmall — p < 2^32: 32-bit products and a 64-bit Barrett step.
+// All return the exact residue, so every kernel built on them is bit-exact.
 #pragma once
 #include <cstdint>
 
@@ -72,9 +73,36 @@ struct FpBarrett {
   }
   MODLIN_HD uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + p - b; }
   MODLIN_HD uint64_t mul(uint64_t a, uint64_t b) const { return reduce((u128)a * b); }
+  // Full product of two residues, for lazy accumulation.
+  MODLIN_HD u128 prod(uint64_t a, uint64_t b) const { return (u128)a * b; }
   // Number of (p-1)^2 products a u128 accumulator holds before it must be reduced.
   MODLIN_HD uint64_t safe_batch() const { return sb; }
   MODLIN_HD uint64_t modulus() const { return p; }
+};
+
+// p < 2^32: residues fit in 32 bits, so a product is one 32x32->64 multiply
+// and a single product reduces with the 64-bit half of the Barrett
+// reciprocal: q = hi64(x * mu_hi) is at most 2 below floor(x / p).
+struct FpSmall {
+  FpBarrett wide;  // reduction of u128 accumulators
+  FpSmall() = default;
+  MODLIN_HD explicit FpSmall(const FieldParams& f) : wide(f) {}
+  MODLIN_HD uint64_t reduce(u128 t) const { return wide.reduce(t); }
+  MODLIN_HD uint64_t reduce64(uint64_t x) const {
+    const uint64_t q = (uint64_t)(((u128)x * wide.mu_hi) >> 64);
+    uint64_t r = x - q * wide.p;
+    if (r >= wide.p) r -= wide.p;
+    if (r >= wide.p) r -= wide.p;
+    return r;
+  }
+  MODLIN_HD uint64_t add(uint64_t a, uint64_t b) const { return wide.add(a, b); }
+  MODLIN_HD uint64_t sub(uint64_t a, uint64_t b) const { return wide.sub(a, b); }
+  MODLIN_HD uint64_t mul(uint64_t a, uint64_t b) const {
+    return reduce64((uint64_t)(uint32_t)a * (uint32_t)b);
+  }
+  MODLIN_HD u128 prod(uint64_t a, uint64_t b) const { return (u128)((uint64_t)(uint32_t)a * (uint32_t)b); }
+  MODLIN_HD uint64_t safe_batch() const { return wide.sb; }
+  MODLIN_HD uint64_t modulus() const { return wide.p; }
 };
 
 struct FpM61 {
@@ -104,6 +132,7 @@ struct FpM61 {
     x = fold(x);
     return x >= kM61 ? x - kM61 : x;
   }
+  MODLIN_HD u128 prod(uint64_t a, uint64_t b) const { return (u128)a * b; }
   MODLIN_HD uint64_t safe_batch() const { return 64; }
   MODLIN_HD uint64_t modulus() const { return kM61; }
 };
@@ -122,6 +151,33 @@ MODLIN_HD uint64_t fp_pow(const F& f, uint64_t a, uint64_t e) {
 template <class F>
 MODLIN_HD uint64_t fp_inv(const F& f, uint64_t a) {
   return fp_pow(f, a, f.modulus() - 2);
+}
+
+// Inverse of a (0 < a < p, p prime) by the binary extended Euclidean
+// algorithm: invariants x1 * a = u and x2 * a = v (mod p), halving u or v and
+// subtracting the smaller from the larger until one reaches 1. About
+// 2 log2(p) short steps, against ~2 log2(p) dependent multiplications for
+// Fermat; used where one thread computes an inverse while the others wait.
+MODLIN_HD uint64_t fp_inv_binary(uint64_t a, uint64_t p) {
+  uint64_t u = a, v = p, x1 = 1, x2 = 0;
+  while (u != 1 && v != 1) {
+    while ((u & 1) == 0) {
+      u >>= 1;
+      x1 = (x1 & 1) ? (x1 + p) >> 1 : x1 >> 1;  // x1 + p < 2^64 for p < 2^63
+    }
+    while ((v & 1) == 0) {
+      v >>= 1;
+      x2 = (x2 & 1) ? (x2 + p) >> 1 : x2 >> 1;
+    }
+    if (u >= v) {
+      u -= v;
+      x1 = x1 >= x2 ? x1 - x2 : x1 + p - x2;
+    } else {
+      v -= u;
+      x2 = x2 >= x1 ? x2 - x1 : x2 + p - x1;
+    }
+  }
+  return u == 1 ? x1 : x2;
 }
 
 }  // namespace modlin

@@ -1,0 +1,241 @@
+// Batched rank: thousands of matrices of uneven sides and primes in one
+// persistent launch (the CLI's `reps` loop, src/main.rs:82, with every job
+// in flight at once).
+//
+// One CTA eliminates one matrix at a time, pulling jobs (largest first) from a
+// device counter. The method is the reference's blocked elimination
+// (src/fp.rs:125-255) with PANEL = 64:
+//   A. in-panel elimination: per column, the first nonzero row at or below
+//      the current rank is the pivot (src/fp.rs:151-156); the row order is a
+//      logical permutation in shared memory instead of physical swaps
+//      (src/fp.rs:158-162); each row below stores its multiplier in place of
+//      the eliminated entry (src/fp.rs:169-170) and updates the rest of the
+//      panel (src/fp.rs:171-173);
+//   B. U block: forward substitution among the panel's pivot rows
+//      (src/fp.rs:181-200), done per 64-column tile in shared memory;
+//   C. trailing update: rows below the pivots -= multipliers x U
+//      (src/fp.rs:202-248), 64x64 tiles, u128 accumulators reduced once per
+//      safe_batch products.
+// The rank is the number of pivots; every residue is exact, so the result is
+// the reference's bit for bit.
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "field.cuh"
+#include "rank_batch.cuh"
+
+namespace modlin {
+
+namespace {
+
+constexpr int kT = kRankBatchThreads;  // 256
+constexpr int kNW = kT / 32;
+constexpr int kP = 64;  // panel width
+
+struct BatchSmem {
+  uint64_t LF[kP][kP + 1];  // multipliers of a row tile, or the pivot rows' multipliers F[k][k2]
+  uint64_t Us[kP][kP];      // U block of one 64-column tile
+  uint64_t prow[kP];        // pivot row's panel segment
+  int pcol[kP];
+  int red[kNW];
+  uint64_t inv;
+  int found;
+  long long job;
+};
+
+template <class F>
+__device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const int n, int* perm, BatchSmem& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t p = f.modulus();
+  const uint64_t sb = f.safe_batch();
+  for (int i = tid; i < n; i += kT) perm[i] = i;
+  __syncthreads();
+  int r0 = 0;
+  for (int c0 = 0; c0 < n && r0 < n; c0 += kP) {
+    const int W = min(kP, n - c0);
+    int pb = 0;
+    // ---- A. in-panel elimination ------------------------------------------
+    for (int kk = 0; kk < W && r0 + pb < n; ++kk) {
+      const int c = c0 + kk, r = r0 + pb;
+      int best = INT_MAX;
+      for (int i = r + tid; i < n; i += kT)
+        if (m[(int64_t)perm[i] * n + c] != 0) {
+          best = i;
+          break;
+        }
+      best = __reduce_min_sync(0xffffffffu, best);
+      if (lane == 0) S.red[warp] = best;
+      __syncthreads();
+      if (tid == 0) {
+        int b = INT_MAX;
+        for (int w = 0; w < kNW; ++w) b = min(b, S.red[w]);
+        S.found = b != INT_MAX;
+        if (b != INT_MAX) {
+          const int t = perm[r];
+          perm[r] = perm[b];
+          perm[b] = t;
+          S.pcol[pb] = c;
+          S.inv = fp_inv_binary(m[(int64_t)perm[r] * n + c], p);
+        }
+      }
+      __syncthreads();
+      if (!S.found) continue;
+      const uint64_t* P = m + (int64_t)perm[r] * n + c0;
+      if (tid < W) S.prow[tid] = P[tid];
+      __syncthreads();
+      const uint64_t inv = S.inv;
+      for (int i = r + 1 + warp; i < n; i += kNW) {
+        uint64_t* R = m + (int64_t)perm[i] * n;
+        const uint64_t e = R[c];
+        if (e == 0) continue;
+        const uint64_t fm = f.mul(e, inv);
+        for (int cc = c + 1 + lane; cc < c0 + W; cc += 32) R[cc] = f.sub(R[cc], f.mul(fm, S.prow[cc - c0]));
+        __syncwarp();
+        if (lane == 0) R[c] = fm;
+      }
+      __syncthreads();
+      ++pb;
+    }
+    if (pb == 0) continue;
+    const int jend = c0 + W;
+    if (jend < n && r0 + pb < n) {
+      // ---- B + C. per 64-column tile: U block, then the trailing rows ------
+      const int tx = tid & 15, ty = tid >> 4;
+      for (int ct = jend; ct < n; ct += kP) {
+        // Pivot rows' multipliers F[k][k2] (k2 < k) and their tile of U.
+        for (int idx = tid; idx < pb * pb; idx += kT) {
+          const int k = idx / pb, k2 = idx - k * pb;
+          S.LF[k][k2] = k2 < k ? m[(int64_t)perm[r0 + k] * n + S.pcol[k2]] : 0;
+        }
+        for (int idx = tid; idx < pb * kP; idx += kT) {
+          const int k = idx >> 6, ci = idx & 63;
+          const int cc = ct + ci;
+          S.Us[k][ci] = cc < n ? m[(int64_t)perm[r0 + k] * n + cc] : 0;
+        }
+        __syncthreads();
+        {
+          // U_k -= sum_{k2<k} F[k][k2] U_k2, four threads per column.
+          const int ci = tid >> 2, q = tid & 3;
+          for (int k = 1; k < pb; ++k) {
+            u128 acc = 0;
+            uint64_t tot = 0, cnt = 0;
+            for (int k2 = q; k2 < k; k2 += 4) {
+              acc += f.prod(S.LF[k][k2], S.Us[k2][ci]);
+              if (++cnt == sb) {
+                tot = f.add(tot, f.reduce(acc));
+                acc = 0;
+                cnt = 0;
+              }
+            }
+            uint64_t part = f.add(tot, f.reduce(acc));
+            part = f.add(part, __shfl_xor_sync(0xffffffffu, part, 1));
+            part = f.add(part, __shfl_xor_sync(0xffffffffu, part, 2));
+            if (q == 0) S.Us[k][ci] = f.sub(S.Us[k][ci], part);
+            __syncwarp();
+          }
+        }
+        __syncthreads();
+        for (int rt = r0 + pb; rt < n; rt += kP) {
+          // Multipliers of the row tile: LF[k][ri] = m[row][pcol[k]].
+          for (int idx = tid; idx < pb * kP; idx += kT) {
+            const int ri = idx / pb, k = idx - ri * pb;
+            const int rr = rt + ri;
+            S.LF[k][ri] = rr < n ? m[(int64_t)perm[rr] * n + S.pcol[k]] : 0;
+          }
+          __syncthreads();
+          // A reduced accumulator (< p <= (p-1)^2 + 1) counts as one product,
+          // so sb terms never overflow the u128.
+          u128 acc[4][4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][q] = 0;
+          uint64_t cnt = 0;
+          for (int k = 0; k < pb; ++k) {
+            uint64_t a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = S.LF[k][ty + 16 * i];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = S.Us[k][tx + 16 * q];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) acc[i][q] += f.prod(a[i], b[q]);
+            if (++cnt == sb) {
+#pragma unroll
+              for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[i][q] = f.reduce(acc[i][q]);
+              cnt = 1;
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int rr = rt + ty + 16 * i;
+            if (rr >= n) continue;
+            uint64_t* R = m + (int64_t)perm[rr] * n;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int cc = ct + tx + 16 * q;
+              if (cc < n) R[cc] = f.sub(R[cc], f.reduce(acc[i][q]));
+            }
+          }
+          __syncthreads();
+        }
+      }
+    }
+    r0 += pb;
+  }
+  return r0;
+}
+
+__global__ void __launch_bounds__(kT, 2)
+    rank_batch_kernel(const RankJob* __restrict__ jobs, int64_t count, unsigned long long* next, int64_t* out) {
+  extern __shared__ __align__(16) unsigned char rb_smem[];
+  BatchSmem& S = *reinterpret_cast<BatchSmem*>(rb_smem);
+  int* perm = reinterpret_cast<int*>(rb_smem + sizeof(BatchSmem));
+  for (;;) {
+    if (threadIdx.x == 0) S.job = (long long)atomicAdd(next, 1ULL);
+    __syncthreads();
+    const long long q = S.job;
+    __syncthreads();
+    if (q >= count) break;
+    const RankJob J = jobs[q];
+    const FieldParams fp{J.p, J.mu_lo, J.mu_hi, J.safe_batch};
+    int r;
+    if (J.p == kM61)
+      r = rank_one(FpM61(fp), J.m, (int)J.n, perm, S);
+    else if (J.p < (1ULL << 32))
+      r = rank_one(FpSmall(fp), J.m, (int)J.n, perm, S);
+    else
+      r = rank_one(FpBarrett(fp), J.m, (int)J.n, perm, S);
+    if (threadIdx.x == 0) out[J.slot] = r;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+size_t rank_batch_smem_bytes(int64_t max_n) { return sizeof(BatchSmem) + (size_t)max_n * sizeof(int); }
+
+int rank_batch_blocks_per_sm(int64_t max_n) {
+  const size_t smem = rank_batch_smem_bytes(max_n);
+  cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rank_batch_kernel, kT, smem);
+  return nb;
+}
+
+cudaError_t launch_rank_batch(const RankJob* d_jobs, int64_t count, unsigned long long* d_next, int64_t max_n,
+                              int blocks, int64_t* d_out, cudaStream_t st) {
+  const size_t smem = rank_batch_smem_bytes(max_n);
+  cudaError_t e = cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  rank_batch_kernel<<<blocks, kT, smem, st>>>(d_jobs, count, d_next, d_out);
+  return cudaGetLastError();
+}
+
+}  // namespace modlin

@@ -127,6 +127,18 @@ def rank_batch(items) -> list[int]:
     return [int(out[i]) for i in range(len(arrs))]
 
 
+def rank_batch_device(ps, ptrs, ns, stream: int = 0) -> list[int]:
+    """Device-resident batch: ``ptrs[i]`` points at an ``ns[i]`` x ``ns[i]``
+    matrix mod ``ps[i]`` (clobbered)."""
+    k = len(ptrs)
+    P = (ctypes.c_uint64 * k)(*ps)
+    D = (ctypes.c_void_p * k)(*ptrs)
+    N = (szt * k)(*ns)
+    out = (szt * k)()
+    check(lib().modlin_rank_batch_device(P, D, N, k, out, stream or None), "rank_batch_device")
+    return [int(out[i]) for i in range(k)]
+
+
 def lc_batch(items) -> list[int]:
     """Linear complexities of ``[(p, sequence), ...]`` in one persistent launch."""
     jobs, arrs = _jobs(items)
