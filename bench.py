@@ -578,6 +578,8 @@ def main():
             extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
         # Berlekamp-Massey: the long sequences and the 65536-sequence batch.
         extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128)
+        # Batched rank: 4096 matrices of sides 64..1024 in one launch.
+        extras["rank_batch"] = rank_batch_measure(torch, modlin, steps=1, warmup=1, single_sample=16)
 
     # End to end through the public C ABI with host buffers: pinned host
     # matrix -> modlin_rank (H2D copy + rank + D2H of the result) each step.
