@@ -9,6 +9,10 @@
  * Results are bit-exact: ranks and linear complexities are mathematical
  * invariants and every kernel computes exact residues.
  *
+ * Entry points on device memory take `void *stream`, a cudaStream_t: the
+ * work is queued there, and NULL means the legacy default stream, so work
+ * the caller queued on it (a copy that fills the input, say) comes first.
+ *
  * Return codes: MODLIN_OK (0) or a negative MODLIN_E* code; no entry point
  * aborts the process (the reference panics: src/fp.rs:50-51).
  * Reference citations are file:line inside the modlin crate.

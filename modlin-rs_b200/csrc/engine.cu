@@ -55,6 +55,7 @@ struct Ctx {
   DevBuf mat, lbuf, ubuf, upanel, gmat, pstate, ispiv, moves;
   DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
   DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
+  DevBuf binv;      // block-step status word and the negated block inverse
   PanelState* h_ps = nullptr;
   int2* h_moves = nullptr;
   // linear-complexity workspaces
@@ -106,6 +107,11 @@ static int cuda_rc(cudaError_t e) {
   }
   return MODLIN_ECUDA;
 }
+
+// Device-memory entry points run on the caller's stream; NULL is the legacy
+// default stream, so work the caller queued there (e.g. a copy that fills the
+// input) is ordered before the call.
+static cudaStream_t user_stream(void* s) { return s ? (cudaStream_t)s : cudaStreamLegacy; }
 
 #define CK(expr)                          \
   do {                                    \
@@ -179,11 +185,63 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     return pr;
   };
 
+  int* binv_status = nullptr;
+  uint64_t* Vneg = nullptr;
+  if (tc) {
+    CK(C->binv.ensure(sizeof(int) + (size_t)kPanel * kPanel * 8 + 256));
+    binv_status = C->binv.as<int>();
+    Vneg = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
+  }
+
   int rank = 0, col = 0;
   while (col < n && rank < n) {
     const int jend = std::min(col + kPanel, n);
     const int W = jend - col;
     const int r0 = rank;
+    if (tc && W == kPanel && n - r0 >= kPanel) {
+      // Block step. When the diagonal block P = A[r0 .. r0+64, col .. jend) is
+      // invertible, its rows are this panel's pivot rows and col .. jend its
+      // pivot columns (every panel column is independent of the earlier
+      // ones); the rows below get the multipliers H = X_P * P^-1 and the
+      // trailing block becomes the Schur complement
+      // A[r0+64.., jend..] - H * A[r0 .. r0+64, jend..], whose rank is the
+      // rank of what remains — the same elimination as the reference's
+      // panel, with both products on the tensor cores and no row moves.
+      CK(cudaMemsetAsync(binv_status, 0, sizeof(int), st));
+      launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st);
+      g_launches += 2;
+      CK(cudaGetLastError());
+      int* h_status = reinterpret_cast<int*>(C->h_out);
+      CK(cudaMemcpyAsync(h_status, binv_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (*h_status == 0) {
+        const int rows = n - r0 - kPanel;
+        if (rows > 0) {
+          CK(cudaMemsetAsync(Lbuf + (size_t)kPanel * kPanel, 0, (size_t)rows * kPanel * 8, st));
+          // H (Lbuf rows 64 .. n - r0, relative to r0) = X_P * P^-1, as
+          // 0 - X_P * (-P^-1).
+          CK(launch_trailing_tc(*R.fp, Lbuf, kPanel, kPanel, n - r0, 0, kPanel, R.m + (int64_t)r0 * ld + col, ld, 0,
+                                Vneg, kPanel, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms,
+                                C->tcerr.as<int>(), st));
+          g_launches += 4;
+          if (jend < n) {
+            auto evp = take_events();
+            cudaEventRecord(evp.first, st);
+            CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + kPanel, n, jend, n, Lbuf, kPanel, r0, R.m + (int64_t)r0 * ld,
+                                  ld, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms,
+                                  C->tcerr.as<int>(), st));
+            cudaEventRecord(evp.second, st);
+            g_launches += 3;
+          }
+        }
+        if (R.pcols)
+          for (int k = 0; k < kPanel; ++k) R.pcols->push_back(col + k);
+        rank += kPanel;
+        col = jend;
+        if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
+        continue;
+      }
+    }
     CK(cudaMemsetAsync(ps, 0, sizeof(PanelState), st));
     g_launches++;
     int round = 0, pb_lo = 0;
@@ -230,7 +288,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       auto evp = take_events();
       cudaEventRecord(evp.first, st);
       if (tc) {
-        CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, n, Lbuf, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
+        CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, n, Lbuf, kPanel, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
                               C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
         g_launches += 3;
       } else {
@@ -480,7 +538,7 @@ int modlin_rank_device(uint64_t p, uint64_t* d_m, size_t n, const modlin_rank_op
   if (rc) return rc;
   if (!d_m) return MODLIN_EINVAL_ARG;
   std::lock_guard<std::mutex> g(C->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  cudaStream_t st = user_stream(stream);
   return rank_device_locked(C, p, d_m, n, opts, rank_out, pivot_cols_out, st, nullptr, nullptr);
 }
 
@@ -495,7 +553,7 @@ int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t 
   int rc = get_ctx(&C);
   if (rc) return rc;
   std::lock_guard<std::mutex> g(C->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  cudaStream_t st = user_stream(stream);
   if (kernel == MODLIN_RANK_PLAIN) {
     if (p == kM61)
       launch_trailing_plain<FpM61>(FpM61(fp), d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U, (int64_t)ldu,
@@ -510,7 +568,7 @@ int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t 
     CK(C->tcB.ensure(tc_b_bytes((int)N)));
     CK(C->tcerr.ensure(2 * sizeof(int)));
     CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
-    CK(launch_trailing_tc(fp, d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U, (int64_t)ldu, (int)K,
+    CK(launch_trailing_tc(fp, d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, kPanel, 0, d_U, (int64_t)ldu, (int)K,
                           C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
     g_launches += 3;
     int err = 0;
@@ -549,7 +607,7 @@ int modlin_linear_complexity_device(uint64_t p, const uint64_t* d_s, size_t n, c
   if (rc) return rc;
   if (!d_s && n) return MODLIN_EINVAL_ARG;
   std::lock_guard<std::mutex> g(C->mu);
-  return lc_device_locked(C, p, d_s, n, opts, lc_out, stream ? (cudaStream_t)stream : C->stream);
+  return lc_device_locked(C, p, d_s, n, opts, lc_out, user_stream(stream));
 }
 
 int modlin_linear_complexity_ex(uint64_t p, const uint64_t* s, size_t n, const modlin_lc_opts* opts,
@@ -585,7 +643,7 @@ int modlin_lc_batch_device(const uint64_t* p, const uint64_t* const* d_data, con
   int rc = get_ctx(&C);
   if (rc) return rc;
   std::lock_guard<std::mutex> g(C->mu);
-  return lc_batch_locked(C, p, d_data, n, count, lcs_out, stream ? (cudaStream_t)stream : C->stream);
+  return lc_batch_locked(C, p, d_data, n, count, lcs_out, user_stream(stream));
 }
 
 int modlin_lc_batch(const modlin_job* jobs, size_t count, size_t* lcs_out) {
@@ -628,7 +686,7 @@ int modlin_rank_batch_device(const uint64_t* p, uint64_t* const* d_m, const size
   int rc = get_ctx(&C);
   if (rc) return rc;
   std::unique_lock<std::mutex> g(C->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  cudaStream_t st = user_stream(stream);
   return rank_batch_locked(C, p, d_m, n, count, ranks_out, st, g);
 }
 
@@ -740,7 +798,7 @@ int modlin_gen_planted_batch_device(const uint64_t* p, const size_t* L, const ui
   int rc = get_ctx(&C);
   if (rc) return rc;
   std::lock_guard<std::mutex> g(C->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  cudaStream_t st = user_stream(stream);
   size_t total_a = 0;
   for (size_t i = 0; i < njobs; ++i) {
     FieldParams fp;
@@ -796,7 +854,7 @@ int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t* d_out, size_t
   int rc = get_ctx(&C);
   if (rc) return rc;
   uint64_t nl = 0;
-  cudaError_t e = gen_uniform_device(p, seed, d_out, count, stream ? (cudaStream_t)stream : C->stream, &nl);
+  cudaError_t e = gen_uniform_device(p, seed, d_out, count, user_stream(stream), &nl);
   g_launches += nl;
   return cuda_rc(e);
 }
@@ -807,7 +865,7 @@ int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) 
   Ctx* C = nullptr;
   int rc = get_ctx(&C);
   if (rc) return rc;
-  cudaStream_t st = stream ? (cudaStream_t)stream : C->stream;
+  cudaStream_t st = user_stream(stream);
   CK(reduce_device(fp, d_x, count, st));
   g_launches++;
   return cuda_rc(cudaStreamSynchronize(st));

@@ -327,6 +327,79 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
 }
 
 // ---------------------------------------------------------------------------
+// block_inverse_kernel — one CTA of 1024 threads: the inverse of the 64 x 64
+// block P = A[r0 .. r0+64, col .. col+64) by fraction-free Gauss-Jordan on
+// [P | I] in shared memory (row j <- e * row j - h * pivot row, one reduction
+// of the two-product sum per entry), or status = 1 when P is singular.
+// Output: Vneg[c][i] = -(P^-1)[c][i] (row c = panel column, column i =
+// block row), the B operand of the multiplier GEMM H = X_P * P^-1.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
+                                                                     int32_t r0, int32_t col,
+                                                                     uint64_t* __restrict__ Vneg, int* status) {
+  extern __shared__ __align__(16) uint64_t smem_inv[];
+  uint64_t(*A)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv);
+  uint64_t(*B)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv + kPanel * (kPanel + 1));
+  __shared__ uint64_t d[kPanel], dinv[kPanel];
+  __shared__ int32_t used[kPanel], pc[kPanel];
+  __shared__ int32_t sh_piv;
+  const uint64_t p = f.modulus();
+  const int tid = threadIdx.x, j = tid >> 4, s = tid & 15;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int c = s + 16 * q;
+    A[j][c] = m[(int64_t)(r0 + j) * ld + col + c];
+    B[j][c] = j == c;
+  }
+  if (s == 0) {
+    used[j] = 0;
+    d[j] = 0;
+  }
+  __syncthreads();
+  for (int c = 0; c < kPanel; ++c) {
+    if (tid < 32) {
+      const bool lo = !used[tid] && A[tid][c] != 0, hi = !used[tid + 32] && A[tid + 32][c] != 0;
+      const uint32_t b0 = __ballot_sync(0xffffffffu, lo), b1 = __ballot_sync(0xffffffffu, hi);
+      if (tid == 0) sh_piv = b0 ? __ffs(b0) - 1 : (b1 ? 31 + __ffs(b1) : -1);
+    }
+    __syncthreads();
+    const int piv = sh_piv;
+    if (piv < 0) {
+      if (tid == 0) *status = 1;
+      return;
+    }
+    const uint64_t e = A[piv][c];
+    const uint64_t h = j != piv ? A[j][c] : 0;
+    if (h != 0) {
+      const uint64_t nh = p - h;
+      for (int cc = c + 1 + s; cc < kPanel; cc += 16) A[j][cc] = f.reduce(f.prod(e, A[j][cc]) + f.prod(nh, A[piv][cc]));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = s + 16 * q;
+        const uint64_t bp = B[piv][k], bj = B[j][k];
+        if (bp | bj) B[j][k] = f.reduce(f.prod(e, bj) + f.prod(nh, bp));
+      }
+      if (s == 0 && used[j]) d[j] = f.mul(e, d[j]);
+    }
+    if (j == piv && s == 0) {
+      used[j] = 1;
+      pc[j] = c;
+      d[j] = e;
+    }
+    __syncthreads();
+  }
+  if (tid < kPanel) dinv[tid] = fp_inv_binary(d[tid], p);
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int k = s + 16 * q;
+    const uint64_t v = f.mul(B[j][k], dinv[j]);
+    Vneg[(int64_t)pc[j] * kPanel + k] = v ? p - v : 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Launch wrappers (explicit instantiation for both field policies).
 // ---------------------------------------------------------------------------
 template <class F>
@@ -388,7 +461,21 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int re
   trailing_plain_kernel<F><<<grid, 256, 0, st>>>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K);
 }
 
+template <class F>
+void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
+                          cudaStream_t st) {
+  const size_t smem = 2 * kPanel * (kPanel + 1) * sizeof(uint64_t);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(block_inverse_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  block_inverse_kernel<F><<<1, kInvThreads, smem, st>>>(f, m, ld, r0, col, Vneg, status);
+}
+
 #define INSTANTIATE(F)                                                                                          \
+  template void launch_block_inverse<F>(const F&, const uint64_t*, int64_t, int, int, uint64_t*, int*,          \
+                                        cudaStream_t);                                                          \
   template void launch_window<F>(const F&, const uint64_t*, int64_t, int, int, int, int, int, PanelState*,       \
                                  uint64_t*, uint64_t*, const uint64_t*, uint8_t*, cudaStream_t);                \
   template void launch_bulk<F>(const F&, uint64_t*, int64_t, int, int, int, int, int, PanelState*,              \

@@ -9,6 +9,11 @@
 
 namespace modlin {
 
+// Inverse of the 64 x 64 diagonal block (negated, row = panel column) or
+// *status = 1 when it is singular.
+template <class F>
+void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
+                          cudaStream_t st);
 template <class F>
 void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
                    PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,

@@ -36,6 +36,7 @@ namespace modlin {
 constexpr int kPanel = 64;         // panel width (src/fp.rs:29)
 constexpr int kWindow = 64;        // candidate rows per window round
 constexpr int kWindowThreads = 512;
+constexpr int kInvThreads = 1024;   // block_inverse_kernel: 16 threads per block row
 
 // Device-resident panel state (one per rank job).
 struct PanelState {

@@ -193,8 +193,8 @@ struct Sched {
 // Limb split of L (A operand): Aw[mt][i][g][kc][rr][kb], thread per (row, kc).
 // ---------------------------------------------------------------------------
 template <int LIMBS>
-__global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int32_t r0, int32_t rbeg, int32_t rend, int32_t K,
-                               int32_t mpad, uint8_t* __restrict__ Aw) {
+__global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, int32_t r0, int32_t rbeg, int32_t rend,
+                               int32_t K, int32_t mpad, uint8_t* __restrict__ Aw) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)mpad * 4) return;
   const int ri_all = (int)(idx >> 2), kc = (int)(idx & 3);
@@ -204,7 +204,7 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int32_t r0, in
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
     const int k = kc * 16 + q;
-    v[q] = (r < rend && k < K) ? Lbuf[(r - r0) * 64 + k] : 0;
+    v[q] = (r < rend && k < K) ? Lbuf[(r - r0) * lda + k] : 0;
   }
   const int64_t tile_off = ((int64_t)mt * LIMBS) * kTileBytes + (((ri >> 3) * 4 + kc) * 8 + (ri & 7)) * 16;
 #pragma unroll
@@ -626,14 +626,14 @@ int limbs_for(uint64_t p) {
 }
 
 template <class F, int LIMBS>
-cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint64_t* Lbuf, int r0,
-                     const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw, uint8_t* Bw, int num_sms, uint64_t r64,
-                     int* err, cudaStream_t st) {
+cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint64_t* Lbuf,
+                     int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw, uint8_t* Bw, int num_sms,
+                     uint64_t r64, int* err, cudaStream_t st) {
   using SH = Shape<LIMBS>;
   const int M = rend - rbeg, N = cend - jend;
   const int mtiles = (M + 127) / 128, nsub = (N + SH::NS - 1) / SH::NS;
   const int mpad = mtiles * 128, npad = nsub * SH::NS;
-  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(Lbuf, r0, rbeg, rend, K, mpad, Aw);
+  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(Lbuf, lda, r0, rbeg, rend, K, mpad, Aw);
   split_b_kernel<LIMBS><<<(npad * 4 + 255) / 256, 256, 0, st>>>(Ubuf, ldU, jend, cend, K, npad, Bw);
   Sched S;
   S.mtiles = mtiles;
@@ -657,21 +657,21 @@ size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc
 size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kK * 8; }
 
 cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
-                               const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw,
-                               uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
+                               const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
+                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
   if (rbeg >= rend || jend >= cend || K <= 0) return cudaSuccess;
   if (K > tc::kK) return cudaErrorInvalidValue;
   const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
   const int L = tc::limbs_for(fp.p);
   if (fp.p == kM61)
-    return tc::launch_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err,
+    return tc::launch_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err,
                                   st);
   const FpBarrett f(fp);
   switch (L) {
-    case 1: return tc::launch_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    case 2: return tc::launch_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    case 4: return tc::launch_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    default: return tc::launch_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    case 1: return tc::launch_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    case 2: return tc::launch_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    case 4: return tc::launch_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
+    default: return tc::launch_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
   }
 }
 

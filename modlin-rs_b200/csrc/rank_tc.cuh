@@ -15,11 +15,11 @@ int tc_crossover_n(uint64_t p);
 size_t tc_a_bytes(int rows);
 size_t tc_b_bytes(int cols);
 // A[rbeg..rend, jend..cend] -= L * U mod p via exact INT8-limb GEMMs (L row
-// r at Lbuf[(r - r0) * 64], U row k at Ubuf[k * ldU], absolute columns). `err` points
+// r at Lbuf[(r - r0) * lda], U row k at Ubuf[k * ldU], absolute columns). `err` points
 // at two device ints (zeroed by the caller); err[0] != 0 afterwards means a
 // bounded wait inside the kernel expired.
 cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
-                               const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw,
-                               uint8_t* Bw, int num_sms, int* err, cudaStream_t st);
+                               const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
+                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st);
 
 }  // namespace modlin
