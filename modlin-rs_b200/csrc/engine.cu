@@ -55,7 +55,10 @@ struct Ctx {
   DevBuf mat, lbuf, ubuf, upanel, gmat, pstate, ispiv, moves;
   DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
   DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
-  DevBuf binv;      // block-step status word and the negated block inverse
+  DevBuf binv;      // block-step status words and the negated block inverse
+  DevBuf tcBn;      // limb planes of the look-ahead (next panel) columns
+  cudaStream_t aux = nullptr;  // look-ahead stream: the next block's inverse
+  cudaEvent_t ev_narrow = nullptr, ev_inv = nullptr;
   PanelState* h_ps = nullptr;
   int2* h_moves = nullptr;
   // linear-complexity workspaces
@@ -185,12 +188,23 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     return pr;
   };
 
+  // Block-step state: two status words (this panel, look-ahead), the
+  // negated block inverse, and the look-ahead result for the next panel
+  // (-1: none, 0: invertible, 1: singular).
   int* binv_status = nullptr;
   uint64_t* Vneg = nullptr;
+  int* h_status = reinterpret_cast<int*>(C->h_out);
+  int pre_status = -1;
   if (tc) {
-    CK(C->binv.ensure(sizeof(int) + (size_t)kPanel * kPanel * 8 + 256));
+    CK(C->binv.ensure(256 + (size_t)kPanel * kPanel * 8));
+    CK(C->tcBn.ensure(tc_b_bytes(kPanel)));
     binv_status = C->binv.as<int>();
     Vneg = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
+    if (!C->aux) {
+      CK(cudaStreamCreateWithFlags(&C->aux, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&C->ev_narrow, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&C->ev_inv, cudaEventDisableTiming));
+    }
   }
 
   int rank = 0, col = 0;
@@ -207,14 +221,21 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       // A[r0+64.., jend..] - H * A[r0 .. r0+64, jend..], whose rank is the
       // rank of what remains — the same elimination as the reference's
       // panel, with both products on the tensor cores and no row moves.
-      CK(cudaMemsetAsync(binv_status, 0, sizeof(int), st));
-      launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st);
-      g_launches += 2;
-      CK(cudaGetLastError());
-      int* h_status = reinterpret_cast<int*>(C->h_out);
-      CK(cudaMemcpyAsync(h_status, binv_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      if (*h_status == 0) {
+      // Look-ahead: the next panel's 64 columns are updated first, and the
+      // next block's inverse runs on a second stream (on the SM the wide
+      // update leaves free) while the rest of the trailing block updates.
+      int status = pre_status;
+      pre_status = -1;
+      if (status < 0) {
+        CK(cudaMemsetAsync(binv_status, 0, sizeof(int), st));
+        launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st);
+        g_launches += 2;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h_status, binv_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        status = h_status[0];
+      }
+      if (status == 0) {
         const int rows = n - r0 - kPanel;
         if (rows > 0) {
           CK(cudaMemsetAsync(Lbuf + (size_t)kPanel * kPanel, 0, (size_t)rows * kPanel * 8, st));
@@ -225,13 +246,38 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
                                 C->tcerr.as<int>(), st));
           g_launches += 4;
           if (jend < n) {
+            const uint64_t* Ub = R.m + (int64_t)r0 * ld;  // the pivot rows
             auto evp = take_events();
             cudaEventRecord(evp.first, st);
-            CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + kPanel, n, jend, n, Lbuf, kPanel, r0, R.m + (int64_t)r0 * ld,
-                                  ld, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms,
-                                  C->tcerr.as<int>(), st));
+            CK(tc_split_a(*R.fp, Lbuf, kPanel, r0, r0 + kPanel, n, kPanel, C->tcA.as<uint8_t>(), st));
+            const bool ahead = jend + kPanel <= n && n - (r0 + kPanel) >= kPanel;
+            int cw = jend;
+            if (ahead) {
+              CK(tc_split_b(*R.fp, Ub, ld, jend, jend + kPanel, kPanel, C->tcBn.as<uint8_t>(), st));
+              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, jend, jend + kPanel, C->tcA.as<uint8_t>(),
+                           C->tcBn.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
+              CK(cudaEventRecord(C->ev_narrow, st));
+              CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
+              CK(cudaMemsetAsync(binv_status + 1, 0, sizeof(int), C->aux));
+              launch_block_inverse<F>(f, R.m, ld, r0 + kPanel, jend, Vneg, binv_status + 1, C->aux);
+              CK(cudaMemcpyAsync(h_status + 1, binv_status + 1, sizeof(int), cudaMemcpyDeviceToHost, C->aux));
+              CK(cudaEventRecord(C->ev_inv, C->aux));
+              g_launches += 4;
+              cw = jend + kPanel;
+            }
+            if (cw < n) {
+              CK(tc_split_b(*R.fp, Ub, ld, cw, n, kPanel, C->tcB.as<uint8_t>(), st));
+              // One SM left to the look-ahead inverse.
+              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, cw, n, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(),
+                           ahead ? C->num_sms - 1 : C->num_sms, C->tcerr.as<int>(), st));
+              g_launches += 2;
+            }
             cudaEventRecord(evp.second, st);
-            g_launches += 3;
+            g_launches += 1;
+            if (ahead) {
+              CK(cudaEventSynchronize(C->ev_inv));
+              pre_status = h_status[1];
+            }
           }
         }
         if (R.pcols)

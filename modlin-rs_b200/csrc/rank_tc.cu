@@ -625,28 +625,34 @@ int limbs_for(uint64_t p) {
   return bits <= 8 ? 1 : bits <= 16 ? 2 : bits <= 32 ? 4 : 8;
 }
 
+template <int LIMBS>
+void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K, uint8_t* Aw, cudaStream_t st) {
+  const int mpad = ((rend - rbeg + 127) / 128) * 128;
+  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(A, lda, r0, rbeg, rend, K, mpad, Aw);
+}
+
+template <int LIMBS>
+void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw, cudaStream_t st) {
+  constexpr int NS = Shape<LIMBS>::NS;
+  const int npad = ((cend - jend + NS - 1) / NS) * NS;
+  split_b_kernel<LIMBS><<<(npad * 4 + 255) / 256, 256, 0, st>>>(B, ldb, jend, cend, K, npad, Bw);
+}
+
 template <class F, int LIMBS>
-cudaError_t launch_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint64_t* Lbuf,
-                     int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K, uint8_t* Aw, uint8_t* Bw, int num_sms,
-                     uint64_t r64, int* err, cudaStream_t st) {
+void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint8_t* Aw,
+              const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st) {
   using SH = Shape<LIMBS>;
-  const int M = rend - rbeg, N = cend - jend;
-  const int mtiles = (M + 127) / 128, nsub = (N + SH::NS - 1) / SH::NS;
-  const int mpad = mtiles * 128, npad = nsub * SH::NS;
-  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(Lbuf, lda, r0, rbeg, rend, K, mpad, Aw);
-  split_b_kernel<LIMBS><<<(npad * 4 + 255) / 256, 256, 0, st>>>(Ubuf, ldU, jend, cend, K, npad, Bw);
   Sched S;
-  S.mtiles = mtiles;
-  S.nsub = nsub;
-  const int64_t total = (int64_t)mtiles * nsub;
-  const int grid = total < num_sms ? (int)total : num_sms;  // one CTA per SM: it owns all 512 TMEM columns
+  S.mtiles = (rend - rbeg + 127) / 128;
+  S.nsub = (cend - jend + SH::NS - 1) / SH::NS;
+  const int64_t total = (int64_t)S.mtiles * S.nsub;
+  const int grid = total < max_ctas ? (int)total : max_ctas;  // one CTA per SM: it owns all 512 TMEM columns
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
     attr = true;
   }
   trailing_tc_kernel<F, LIMBS><<<grid, kThreads, SH::SMEM, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64, err);
-  return cudaGetLastError();
 }
 
 }  // namespace tc
@@ -656,23 +662,59 @@ int tc_crossover_n(uint64_t) { return 512; }
 size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc::kK * 8; }
 size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kK * 8; }
 
+cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
+                       uint8_t* Aw, cudaStream_t st) {
+  if (rbeg >= rend) return cudaSuccess;
+  if (K <= 0 || K > tc::kK) return cudaErrorInvalidValue;
+  switch (fp.p == kM61 ? 8 : tc::limbs_for(fp.p)) {
+    case 1: tc::split_a_t<1>(A, lda, r0, rbeg, rend, K, Aw, st); break;
+    case 2: tc::split_a_t<2>(A, lda, r0, rbeg, rend, K, Aw, st); break;
+    case 4: tc::split_a_t<4>(A, lda, r0, rbeg, rend, K, Aw, st); break;
+    default: tc::split_a_t<8>(A, lda, r0, rbeg, rend, K, Aw, st); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
+                       cudaStream_t st) {
+  if (jend >= cend) return cudaSuccess;
+  if (K <= 0 || K > tc::kK) return cudaErrorInvalidValue;
+  switch (fp.p == kM61 ? 8 : tc::limbs_for(fp.p)) {
+    case 1: tc::split_b_t<1>(B, ldb, jend, cend, K, Bw, st); break;
+    case 2: tc::split_b_t<2>(B, ldb, jend, cend, K, Bw, st); break;
+    case 4: tc::split_b_t<4>(B, ldb, jend, cend, K, Bw, st); break;
+    default: tc::split_b_t<8>(B, ldb, jend, cend, K, Bw, st); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st) {
+  if (rbeg >= rend || jend >= cend) return cudaSuccess;
+  const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
+  if (fp.p == kM61) {
+    tc::update_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
+  } else {
+    const FpBarrett f(fp);
+    switch (tc::limbs_for(fp.p)) {
+      case 1: tc::update_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
+      case 2: tc::update_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
+      case 4: tc::update_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
+      default: tc::update_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
+    }
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
                                const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
                                uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
   if (rbeg >= rend || jend >= cend || K <= 0) return cudaSuccess;
   if (K > tc::kK) return cudaErrorInvalidValue;
-  const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
-  const int L = tc::limbs_for(fp.p);
-  if (fp.p == kM61)
-    return tc::launch_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err,
-                                  st);
-  const FpBarrett f(fp);
-  switch (L) {
-    case 1: return tc::launch_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    case 2: return tc::launch_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    case 4: return tc::launch_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-    default: return tc::launch_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Lbuf, lda, r0, Ubuf, ldU, K, Aw, Bw, num_sms, r64, err, st);
-  }
+  cudaError_t e = tc_split_a(fp, Lbuf, lda, r0, rbeg, rend, K, Aw, st);
+  if (e == cudaSuccess) e = tc_split_b(fp, Ubuf, ldU, jend, cend, K, Bw, st);
+  if (e == cudaSuccess) e = tc_update(fp, m, ld, rbeg, rend, jend, cend, Aw, Bw, num_sms, err, st);
+  return e;
 }
 
 }  // namespace modlin

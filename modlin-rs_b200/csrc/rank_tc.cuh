@@ -22,4 +22,15 @@ cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, i
                                const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
                                uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st);
 
+// The three steps of launch_trailing_tc, for callers that reuse one operand's
+// limb planes across launches: limb planes of A rows [rbeg, rend) (row r at
+// A[(r - r0) * lda]), of B columns [jend, cend) (row k at B[k * ldb]), and the
+// update A[rbeg..rend, jend..cend] -= A * B on at most max_ctas SMs.
+cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
+                       uint8_t* Aw, cudaStream_t st);
+cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
+                       cudaStream_t st);
+cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st);
+
 }  // namespace modlin
