@@ -417,6 +417,41 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
     return res
 
 
+def rank_planted_measure(torch, modlin, n=16384, L=4096, seed=8, steps=1):
+    """The planted large rank: rows are successive length-n windows of an
+    order-L recurrence from SplitMix64(seed), so the rank is L (pivot columns
+    0..L-1) and everything after the first L columns is eliminated to zero.
+    Both trailing kernels, one rank each per step, ranks and column profiles
+    checked."""
+    from modlin import fp as mfp
+    pristine = torch.empty(n * n, dtype=torch.int64, device="cuda")
+    t0 = time.perf_counter()
+    modlin.gen.planted_device(M61, L, seed, pristine.data_ptr(), n * n)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    work = torch.empty_like(pristine)
+    W = sum((n - 1 - k) ** 2 for k in range(L))
+    res = {"n": n, "order": L, "work_modmac": W, "generation_s": gen_s}
+    for kern in ("tc", "plain"):
+        work.copy_(pristine)
+        r, pc = mfp.rank_device(M61, work.data_ptr(), n, kernel=kern, pivot_cols=True)
+        assert r == L and list(pc) == list(range(L)), (kern, r)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = 0.0
+        for _ in range(steps):
+            work.copy_(pristine)
+            e0.record()
+            assert mfp.rank_device(M61, work.data_ptr(), n, kernel=kern) == L
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms /= steps
+        res[kern] = {"rank": r, "corank": n - r, "ms": ms, "modmac_per_s": W / (ms * 1e-3)}
+    res["tc_speedup_vs_plain"] = res["tc"]["modmac_per_s"] / res["plain"]["modmac_per_s"]
+    del work, pristine
+    return res
+
+
 def host_cores():
     try:
         import oracle
@@ -475,7 +510,7 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
-    ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch"],
+    ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch", "rank-planted"],
                     help="rank: the 16384^2 rank (default line); bm / rank-batch: only those measurements")
     args = ap.parse_args()
 
@@ -500,6 +535,11 @@ def main():
         res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
         if rank == 0:
             print(json.dumps({"workload": "berlekamp-massey", **res}), flush=True)
+        return
+    if args.workload == "rank-planted":
+        res = rank_planted_measure(torch, modlin, steps=args.steps)
+        if rank == 0:
+            print(json.dumps({"workload": "planted large rank", **res}), flush=True)
         return
     if args.workload == "rank-batch":
         res = rank_batch_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
@@ -578,6 +618,8 @@ def main():
             extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
         # Berlekamp-Massey: the long sequences and the 65536-sequence batch.
         extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128)
+        # The planted large rank (order-4096 recurrence windows, rank 4096).
+        extras["rank_planted"] = rank_planted_measure(torch, modlin)
         # Batched rank: 4096 matrices of sides 64..1024 in one launch.
         extras["rank_batch"] = rank_batch_measure(torch, modlin, steps=1, warmup=1, single_sample=16)
 

@@ -64,6 +64,7 @@ struct Ctx {
   // linear-complexity workspaces
   DevBuf seq, bmws, bmout, bmsync, bmjobs, bmnext;
   DevBuf gena, genjobs;  // planted-generator coefficients and jobs
+  DevBuf jump;           // jump-ahead scratch of the long planted generator
   DevBuf batchm, rbjobs, rbout;  // batched rank: matrix arena, jobs, ranks
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
@@ -890,7 +891,67 @@ int modlin_gen_planted_batch_device(const uint64_t* p, const size_t* L, const ui
 }
 
 int modlin_gen_planted_device(uint64_t p, size_t L, uint64_t seed, uint64_t* d_out, size_t count, void* stream) {
-  return modlin_gen_planted_batch_device(&p, &L, &seed, &d_out, &count, 1, stream);
+  // Long streams of a high-order recurrence: jump-ahead segments extended in
+  // parallel instead of one CTA walking the whole stream.
+  const bool jump = L >= 64 && L <= (1u << 20) && count >= ((size_t)1 << 22) && count >= 256 * L;
+  if (!jump) return modlin_gen_planted_batch_device(&p, &L, &seed, &d_out, &count, 1, stream);
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!d_out) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  cudaStream_t st = user_stream(stream);
+  const int Li = (int)L;
+  int K = (int)std::min<size_t>(1024, count / (64 * L));
+  const int64_t T = (int64_t)((count + K - 1) / K);
+  K = (int)((count + T - 1) / T);
+  std::vector<uint64_t> a, init;
+  draw_planted(p, L, seed, a, init);
+  // Scratch: a (L), head (2L), u (2L), R (K L), xpow (2L), tmp (L), cbuf (2L), qbuf (L).
+  const size_t words = (size_t)L * (1 + 2 + 2 + 2 + 1 + 2 + 1) + (size_t)K * L;
+  CK(C->jump.ensure(words * 8));
+  uint64_t* w = C->jump.as<uint64_t>();
+  uint64_t* d_a = w;
+  uint64_t* head = d_a + L;
+  uint64_t* u = head + 2 * L;
+  uint64_t* xpow = u + 2 * L;
+  uint64_t* tmp = xpow + 2 * L;
+  uint64_t* cbuf = tmp + L;
+  uint64_t* qbuf = cbuf + 2 * L;
+  uint64_t* R = qbuf + L;
+  CK(cudaMemcpyAsync(d_a, a.data() + 1, L * 8, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(head, init.data(), L * 8, cudaMemcpyHostToDevice, st));
+  std::vector<uint64_t> impulse(L, 0);
+  impulse[L - 1] = 1;
+  CK(cudaMemcpyAsync(u, impulse.data(), L * 8, cudaMemcpyHostToDevice, st));
+  // head = s[0 .. 2L-1); u[L-1 ..] = g, the power series 1 / (1 - sum a_j x^j).
+  std::vector<PlantJob> jobs;
+  jobs.push_back(PlantJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_a, head, (int64_t)L, (int64_t)(2 * L - 1)});
+  jobs.push_back(PlantJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_a, u, (int64_t)L, (int64_t)(2 * L - 1)});
+  CK(C->genjobs.ensure(std::max<size_t>(K, 2) * sizeof(PlantJob)));
+  CK(C->bmnext.ensure(sizeof(unsigned long long)));
+  CK(cudaMemcpyAsync(C->genjobs.p, jobs.data(), 2 * sizeof(PlantJob), cudaMemcpyHostToDevice, st));
+  const int threads = L >= 8192 ? 1024 : 512;
+  CK(plant_device(C->genjobs.as<PlantJob>(), 2, C->bmnext.as<unsigned long long>(), 2, threads, st));
+  JumpPlan P{d_a, u + (L - 1), head, d_out, R, xpow, tmp, cbuf, qbuf, Li, K, T, (int64_t)count};
+  CK(jump_states(fp, P, st));
+  // Every segment extended from its state by the recurrence.
+  jobs.clear();
+  for (int k = 0; k < K; ++k) {
+    const int64_t t0 = (int64_t)k * T;
+    const int64_t len = std::min<int64_t>(T, (int64_t)count - t0);
+    jobs.push_back(PlantJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_a, d_out + t0, (int64_t)L, len});
+  }
+  // The job table is read by the device after this host vector is reused:
+  // wait for the first launch's copies before overwriting the table.
+  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpyAsync(C->genjobs.p, jobs.data(), jobs.size() * sizeof(PlantJob), cudaMemcpyHostToDevice, st));
+  const int blocks = std::min<int>(K, C->num_sms * (2048 / threads));
+  CK(plant_device(C->genjobs.as<PlantJob>(), (int64_t)K, C->bmnext.as<unsigned long long>(), blocks, threads, st));
+  g_launches += 6 + 3 * (size_t)(K + 40);
+  return cuda_rc(cudaStreamSynchronize(st));
 }
 
 int modlin_gen_uniform_device(uint64_t p, uint64_t seed, uint64_t* d_out, size_t count, void* stream) {

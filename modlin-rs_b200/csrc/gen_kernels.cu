@@ -241,4 +241,207 @@ cudaError_t plant_device(const PlantJob* d_jobs, int64_t count, unsigned long lo
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Jump-ahead for long planted streams. With f(x) = x^L - sum_j a_j x^(L-j)
+// and the functional phi(x^i) = s[i] (well defined: phi kills multiples of f),
+// s[t + i] = phi(x^t x^i) = sum_j r_j s[j + i] for r = x^t mod f. The stream
+// is cut into K segments; segment k starts from the state computed with
+// r_k = x^(kT) mod f and is then extended by the recurrence, so every value
+// equals the sequential stream's. Polynomial products and remainders mod f
+// run a warp per output coefficient; the remainder uses the reversed-inverse
+// quotient rev(q) = rev(c) * g mod x^(L-1), g = 1 / (1 - sum_j a_j x^j).
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ __forceinline__ uint64_t warp_dot_sum(const F& f, u128 acc, uint64_t tot) {
+  uint64_t v = f.add(tot, f.reduce(acc));
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = f.add(v, __shfl_down_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// c[m] = sum_{i+j=m} a[i] b[j], m < 2L-1.
+template <class F>
+__global__ void poly_mul_kernel(F f, const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
+                                uint64_t* __restrict__ c, int L) {
+  const int m = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (m >= 2 * L - 1) return;
+  const int lo = m - (L - 1) > 0 ? m - (L - 1) : 0, hi = m < L - 1 ? m : L - 1;
+  const uint64_t sb = f.safe_batch();
+  u128 acc = 0;
+  uint64_t tot = 0, cnt = 0;
+  for (int i = lo + lane; i <= hi; i += 32) {
+    acc += f.prod(a[i], b[m - i]);
+    if (++cnt == sb) {
+      tot = f.add(tot, f.reduce(acc));
+      acc = 0;
+      cnt = 0;
+    }
+  }
+  const uint64_t v = warp_dot_sum(f, acc, tot);
+  if (lane == 0) c[m] = v;
+}
+
+// q[L-2-i] = sum_{k<=i} c[2L-2-k] g[i-k], i < L-1 (the quotient c div f).
+template <class F>
+__global__ void poly_quot_kernel(F f, const uint64_t* __restrict__ c, const uint64_t* __restrict__ g,
+                                 uint64_t* __restrict__ q, int L) {
+  const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (i >= L - 1) return;
+  const uint64_t sb = f.safe_batch();
+  u128 acc = 0;
+  uint64_t tot = 0, cnt = 0;
+  for (int k = lane; k <= i; k += 32) {
+    acc += f.prod(c[2 * L - 2 - k], g[i - k]);
+    if (++cnt == sb) {
+      tot = f.add(tot, f.reduce(acc));
+      acc = 0;
+      cnt = 0;
+    }
+  }
+  const uint64_t v = warp_dot_sum(f, acc, tot);
+  if (lane == 0) q[L - 2 - i] = v;
+}
+
+// r[m] = c[m] - (q f)[m] = c[m] + sum_{i<=min(m,L-2)} q[i] a_(L-m+i), m < L
+// (a[] holds a_1..a_L at indices 0..L-1).
+template <class F>
+__global__ void poly_rem_kernel(F f, const uint64_t* __restrict__ c, const uint64_t* __restrict__ q,
+                                const uint64_t* __restrict__ a, uint64_t* __restrict__ r, int L) {
+  const int m = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (m >= L) return;
+  const int hi = m < L - 2 ? m : L - 2;
+  const uint64_t sb = f.safe_batch();
+  u128 acc = 0;
+  uint64_t tot = 0, cnt = 0;
+  for (int i = lane; i <= hi; i += 32) {
+    acc += f.prod(q[i], a[L - 1 - m + i]);
+    if (++cnt == sb) {
+      tot = f.add(tot, f.reduce(acc));
+      acc = 0;
+      cnt = 0;
+    }
+  }
+  const uint64_t v = warp_dot_sum(f, acc, tot);
+  if (lane == 0) r[m] = f.add(c[m], v);
+}
+
+// Segment states: out[k T + i] = sum_{j<L} R[k][j] s[j + i] for i < min(L,
+// count - k T); 64 x 64 output tiles, 4 x 4 per thread, u128 accumulators.
+template <class F>
+__global__ void __launch_bounds__(256) jump_states_kernel(F f, const uint64_t* __restrict__ R,
+                                                          const uint64_t* __restrict__ s, int L, int K, int64_t T,
+                                                          int64_t count, uint64_t* __restrict__ out) {
+  __shared__ uint64_t Rs[32][64 + 1];
+  __shared__ uint64_t Ss[96];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int i0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
+  const uint64_t sb = f.safe_batch();
+  u128 acc[4][4];
+  uint64_t tot[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b] = 0;
+      tot[a][b] = 0;
+    }
+  uint64_t cnt = 0;
+  for (int j0 = 0; j0 < L; j0 += 32) {
+    for (int idx = tid; idx < 32 * 64; idx += 256) {
+      const int kk = idx >> 5, jj = idx & 31;
+      const int k = k0 + kk, j = j0 + jj;
+      Rs[jj][kk] = (k < K && j < L) ? R[(int64_t)k * L + j] : 0;
+    }
+    for (int t = tid; t < 96; t += 256) {
+      const int idx = j0 + i0 + t;
+      Ss[t] = idx < 2 * L - 1 ? s[idx] : 0;
+    }
+    __syncthreads();
+    const int jn = L - j0 < 32 ? L - j0 : 32;
+    for (int jj = 0; jj < jn; ++jj) {
+      uint64_t rv[4], sv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) rv[a] = Rs[jj][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) sv[b] = Ss[jj + tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += f.prod(rv[a], sv[b]);
+      if (++cnt == sb) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            tot[a][b] = f.add(tot[a][b], f.reduce(acc[a][b]));
+            acc[a][b] = 0;
+          }
+        cnt = 0;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int k = k0 + ty + 16 * a;
+    if (k >= K) continue;
+    const int64_t base = (int64_t)k * T;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + tx + 16 * b;
+      if (i < L && base + i < count) out[base + i] = f.add(tot[a][b], f.reduce(acc[a][b]));
+    }
+  }
+}
+
+template <class F>
+static cudaError_t jump_mulmod(const F& f, const uint64_t* x, const uint64_t* y, uint64_t* r, const uint64_t* a,
+                               const uint64_t* g, uint64_t* cbuf, uint64_t* qbuf, int L, cudaStream_t st) {
+  poly_mul_kernel<F><<<(2 * L - 1 + 7) / 8, 256, 0, st>>>(f, x, y, cbuf, L);
+  poly_quot_kernel<F><<<(L - 1 + 7) / 8, 256, 0, st>>>(f, cbuf, g, qbuf, L);
+  poly_rem_kernel<F><<<(L + 7) / 8, 256, 0, st>>>(f, cbuf, qbuf, a, r, L);
+  return cudaGetLastError();
+}
+
+template <class F>
+static cudaError_t jump_states_t(const F& f, const JumpPlan& P, cudaStream_t st) {
+  const int L = P.L;
+  // R[0] = 1, xT = x^T mod f by square-and-multiply from x mod f, then
+  // R[k] = R[k-1] * xT mod f.
+  cudaError_t e = cudaMemsetAsync(P.R, 0, (size_t)P.K * L * 8, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(P.xpow, 0, (size_t)2 * L * 8, st);
+  if (e != cudaSuccess) return e;
+  const uint64_t one = 1;
+  e = cudaMemcpyAsync(P.R, &one, 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(P.xpow + L + 1, &one, 8, cudaMemcpyHostToDevice, st);  // x (L >= 2)
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(P.xpow, &one, 8, cudaMemcpyHostToDevice, st);  // accumulator = 1
+  if (e != cudaSuccess) return e;
+  uint64_t* acc = P.xpow;
+  uint64_t* base = P.xpow + L;
+  int top = 63;
+  while (top > 0 && !((P.T >> top) & 1)) --top;
+  for (int b = top; b >= 0; --b) {
+    e = jump_mulmod(f, acc, acc, P.tmp, P.a, P.g, P.cbuf, P.qbuf, L, st);
+    if (e == cudaSuccess && ((P.T >> b) & 1)) e = jump_mulmod(f, P.tmp, base, acc, P.a, P.g, P.cbuf, P.qbuf, L, st);
+    else if (e == cudaSuccess) e = cudaMemcpyAsync(acc, P.tmp, (size_t)L * 8, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  for (int k = 1; k < P.K; ++k) {
+    e = jump_mulmod(f, P.R + (int64_t)(k - 1) * L, acc, P.R + (int64_t)k * L, P.a, P.g, P.cbuf, P.qbuf, L, st);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 grid((L + 63) / 64, (P.K + 63) / 64);
+  jump_states_kernel<F><<<grid, 256, 0, st>>>(f, P.R, P.head, L, P.K, P.T, P.count, P.out);
+  return cudaGetLastError();
+}
+
+cudaError_t jump_states(const FieldParams& fp, const JumpPlan& P, cudaStream_t st) {
+  if (P.L < 2 || P.K < 1) return cudaErrorInvalidValue;
+  if (fp.p == kM61) return jump_states_t(FpM61(fp), P, st);
+  return jump_states_t(FpBarrett(fp), P, st);
+}
+
 }  // namespace modlin

@@ -23,4 +23,19 @@ struct PlantJob {
 cudaError_t plant_device(const PlantJob* d_jobs, int64_t count, unsigned long long* d_next, int blocks, int threads,
                          cudaStream_t st);
 
+// Segment states of a long planted stream (jump-ahead): with head =
+// s[0 .. 2L-1), writes out[k T .. k T + L) = s[k T .. k T + L) for k < K (cut
+// at count). a = a_1..a_L, g = 1 / (1 - sum_j a_j x^j) mod x^(L-1); R (K x L),
+// xpow (2L), tmp (L), cbuf (2L), qbuf (L) are device scratch. L >= 2.
+struct JumpPlan {
+  const uint64_t* a;
+  const uint64_t* g;
+  const uint64_t* head;
+  uint64_t* out;
+  uint64_t *R, *xpow, *tmp, *cbuf, *qbuf;
+  int L, K;
+  int64_t T, count;
+};
+cudaError_t jump_states(const FieldParams& fp, const JumpPlan& P, cudaStream_t st);
+
 }  // namespace modlin

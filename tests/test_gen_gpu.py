@@ -50,3 +50,17 @@ def test_planted_device_linear_complexity(M):
         t = torch.empty(n, dtype=torch.int64, device="cuda")
         M.gen.planted_device(p, L, 9, t.data_ptr(), n)
         assert M.fp.linear_complexity_device(p, t.data_ptr(), n) == L
+
+
+@pytest.mark.parametrize("p,L,count", [(M61, 64, 1 << 22), (65521, 300, (1 << 22) + 777), (2**63 - 25, 128, 1 << 22)])
+def test_planted_device_jump_ahead_matches_host(M, p, L, count):
+    """Long streams go through the jump-ahead segments (x^T mod f states,
+    segments extended in parallel): every value equals the sequential
+    stream's."""
+    import torch
+    t = torch.empty(count, dtype=torch.int64, device="cuda")
+    M.gen.planted_device(p, L, 77, t.data_ptr(), count)
+    got = t.cpu().numpy().view(np.uint64)
+    want = M.gen.planted(p, L, 77, count)
+    bad = np.flatnonzero(got != want)
+    assert bad.size == 0, (bad[:5], bad.size)
