@@ -98,8 +98,10 @@ int modlin_rank_device(uint64_t p, uint64_t *d_m, size_t n, const modlin_rank_op
 
 /* The trailing update of one panel (src/fp.rs:202-248) as a standalone
  * device operation: C[M x N] -= L[M x K] * U[K x N] (mod p), all entries in
- * [0, p), K <= 64. L has row stride 64, U row stride ldu, C row stride ldc.
- * kernel: MODLIN_RANK_PLAIN or MODLIN_RANK_TC (MODLIN_RANK_AUTO = TC). */
+ * [0, p). K <= 64 (L row stride 64), or with the tensor-core kernel also
+ * K <= 128 (two panels at once; L row stride 128). U has row stride ldu, C
+ * row stride ldc. kernel: MODLIN_RANK_PLAIN or MODLIN_RANK_TC
+ * (MODLIN_RANK_AUTO = TC). */
 int modlin_trailing_update_device(uint64_t p, uint64_t *d_C, size_t ldc, size_t M, size_t N,
                                   const uint64_t *d_L, const uint64_t *d_U, size_t ldu, size_t K,
                                   int kernel, void *stream);

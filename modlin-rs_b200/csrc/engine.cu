@@ -255,7 +255,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
             int cw = jend;
             if (ahead) {
               CK(tc_split_b(*R.fp, Ub, ld, jend, jend + kPanel, kPanel, C->tcBn.as<uint8_t>(), st));
-              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, jend, jend + kPanel, C->tcA.as<uint8_t>(),
+              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, jend, jend + kPanel, kPanel, C->tcA.as<uint8_t>(),
                            C->tcBn.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
               CK(cudaEventRecord(C->ev_narrow, st));
               CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
@@ -269,7 +269,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
             if (cw < n) {
               CK(tc_split_b(*R.fp, Ub, ld, cw, n, kPanel, C->tcB.as<uint8_t>(), st));
               // One SM left to the look-ahead inverse.
-              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, cw, n, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(),
+              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, cw, n, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(),
                            ahead ? C->num_sms - 1 : C->num_sms, C->tcerr.as<int>(), st));
               g_launches += 2;
             }
@@ -593,7 +593,8 @@ int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t 
                                   const uint64_t* d_U, size_t ldu, size_t K, int kernel, void* stream) {
   FieldParams fp;
   if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
-  if (K > (size_t)kPanel || M > 0x3fffffff || N > 0x3fffffff || ldc < N || ldu < N) return MODLIN_EINVAL_N;
+  const size_t kmax = kernel == MODLIN_RANK_PLAIN ? (size_t)kPanel : (size_t)2 * kPanel;
+  if (K > kmax || M > 0x3fffffff || N > 0x3fffffff || ldc < N || ldu < N) return MODLIN_EINVAL_N;
   if ((M && N && K) && (!d_C || !d_L || !d_U)) return MODLIN_EINVAL_ARG;
   if (!M || !N || !K) return MODLIN_OK;
   Ctx* C = nullptr;
@@ -615,7 +616,8 @@ int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t 
     CK(C->tcB.ensure(tc_b_bytes((int)N)));
     CK(C->tcerr.ensure(2 * sizeof(int)));
     CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
-    CK(launch_trailing_tc(fp, d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, kPanel, 0, d_U, (int64_t)ldu, (int)K,
+    const int64_t lda = K <= (size_t)kPanel ? kPanel : 2 * kPanel;
+    CK(launch_trailing_tc(fp, d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, lda, 0, d_U, (int64_t)ldu, (int)K,
                           C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
     g_launches += 3;
     int err = 0;

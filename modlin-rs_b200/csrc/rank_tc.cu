@@ -47,13 +47,10 @@ namespace modlin {
 
 namespace tc {
 
-constexpr int kK = 64;          // K (panel width) of one update, zero padded
-constexpr int kStages = 6;      // B ring depth
-constexpr int kTileBytes = 8192;  // one 128-row x 64-byte limb plane tile
+constexpr int kKMax = 128;      // largest K of one update (two panels), zero padded to 64 or 128
 constexpr int kEpiWarps = 16;                // TMEM-draining warps (4 per lane quadrant)
 constexpr int kThreads = 32 * (2 + kEpiWarps);  // producer warp, MMA warp, epilogue warps
 constexpr uint32_t kTmemCols = 512;  // two accumulator buffers of 256 columns
-constexpr int kCDepth = 4;           // staged C tiles (subtiles) in shared memory
 constexpr int kCStride = 18;         // padded row stride (words) of a staged 128 x 16 C tile (16-byte rows)
 constexpr long long kSpinLimit = 4000000000LL;  // ~2 s at 2 GHz
 
@@ -174,15 +171,24 @@ __device__ __forceinline__ void cp_async_wait() {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-template <int LIMBS>
+// KK = 64 (one panel) or 128 (two panels per pass: half the epilogue work
+// per modMAC). A plane tile is 128 rows x KK bytes in 8-row x 16-byte core
+// matrices; SBO (next 8-row group) = KK * 8 bytes.
+template <int LIMBS, int KK>
 struct Shape {
   static constexpr int NS = 128 / LIMBS;             // output columns per subtile
   static constexpr int DIAG = 2 * LIMBS - 1;         // diagonal accumulators
-  static constexpr int A_BYTES = LIMBS * kTileBytes;  // resident A tile
-  static constexpr int B_BYTES = kTileBytes;         // one B subtile (all planes)
+  static constexpr int TILE = 128 * KK;              // one limb plane tile
+  static constexpr int KC = KK / 16;                 // 16-byte core matrices along K
+  static constexpr uint32_t SBO = KK * 8;
+  static constexpr int STAGES = KK == 64 ? 6 : 3;    // B ring depth
+  static constexpr int CDEPTH = KK == 64 ? 4 : 2;    // staged C tiles (subtiles) in shared memory
+  static constexpr int A_BYTES = LIMBS * TILE;       // resident A tile
+  static constexpr int B_BYTES = TILE;               // one B subtile (all planes)
   static constexpr int ZERO_BYTES = 4096;            // zero A tile (128 x 32 B)
-  static constexpr int C_BYTES = LIMBS == 8 ? kCDepth * 128 * kCStride * 8 : 0;  // staged C tiles
-  static constexpr int SMEM = A_BYTES + kStages * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
+  static constexpr int C_BYTES = LIMBS == 8 ? CDEPTH * 128 * kCStride * 8 : 0;  // staged C tiles
+  static constexpr int SMEM = A_BYTES + STAGES * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
+  static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 struct Sched {
@@ -192,12 +198,13 @@ struct Sched {
 // ---------------------------------------------------------------------------
 // Limb split of L (A operand): Aw[mt][i][g][kc][rr][kb], thread per (row, kc).
 // ---------------------------------------------------------------------------
-template <int LIMBS>
+template <int LIMBS, int KK>
 __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, int32_t r0, int32_t rbeg, int32_t rend,
                                int32_t K, int32_t mpad, uint8_t* __restrict__ Aw) {
+  using SH = Shape<LIMBS, KK>;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)mpad * 4) return;
-  const int ri_all = (int)(idx >> 2), kc = (int)(idx & 3);
+  if (idx >= (int64_t)mpad * SH::KC) return;
+  const int ri_all = (int)(idx / SH::KC), kc = (int)(idx % SH::KC);
   const int mt = ri_all >> 7, ri = ri_all & 127;
   const int64_t r = (int64_t)rbeg + ri_all;
   uint64_t v[16];
@@ -206,7 +213,7 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, i
     const int k = kc * 16 + q;
     v[q] = (r < rend && k < K) ? Lbuf[(r - r0) * lda + k] : 0;
   }
-  const int64_t tile_off = ((int64_t)mt * LIMBS) * kTileBytes + (((ri >> 3) * 4 + kc) * 8 + (ri & 7)) * 16;
+  const int64_t tile_off = ((int64_t)mt * LIMBS) * SH::TILE + (((ri >> 3) * SH::KC + kc) * 8 + (ri & 7)) * 16;
 #pragma unroll
   for (int i = 0; i < LIMBS; ++i) {
     uint32_t w[4];
@@ -217,7 +224,7 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, i
       for (int b = 0; b < 4; ++b) x |= (uint32_t)((v[q4 * 4 + b] >> (8 * i)) & 0xFF) << (8 * b);
       w[q4] = x;
     }
-    *reinterpret_cast<uint4*>(Aw + tile_off + (int64_t)i * kTileBytes) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(Aw + tile_off + (int64_t)i * SH::TILE) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -225,12 +232,13 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, i
 // Limb split of U (B operand): Bw[sub][j][g2][kc][rr][kb], thread per
 // (column, kc); reads Ubuf[k][c] (coalesced over c).
 // ---------------------------------------------------------------------------
-template <int LIMBS>
+template <int LIMBS, int KK>
 __global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, int32_t jend, int32_t cend, int32_t K,
                                int32_t npad, uint8_t* __restrict__ Bw) {
-  constexpr int NS = Shape<LIMBS>::NS;
+  using SH = Shape<LIMBS, KK>;
+  constexpr int NS = SH::NS;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)npad * 4) return;
+  if (idx >= (int64_t)npad * SH::KC) return;
   const int kc = (int)(idx / npad), ci = (int)(idx - (int64_t)kc * npad);
   const int64_t c = (int64_t)jend + ci;
   uint64_t v[16];
@@ -240,7 +248,7 @@ __global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, i
     v[q] = (c < cend && k < K) ? Ubuf[(int64_t)k * ldU + c] : 0;
   }
   const int sub = ci / NS, cc = ci % NS;
-  const int64_t base = (int64_t)sub * kTileBytes + (((cc >> 3) * 4 + kc) * 8 + (cc & 7)) * 16;
+  const int64_t base = (int64_t)sub * SH::TILE + (((cc >> 3) * SH::KC + kc) * 8 + (cc & 7)) * 16;
 #pragma unroll
   for (int j = 0; j < LIMBS; ++j) {
     uint32_t w[4];
@@ -251,7 +259,7 @@ __global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, i
       for (int b = 0; b < 4; ++b) x |= (uint32_t)((v[q4 * 4 + b] >> (8 * j)) & 0xFF) << (8 * b);
       w[q4] = x;
     }
-    *reinterpret_cast<uint4*>(Bw + base + (int64_t)j * NS * kK) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(Bw + base + (int64_t)j * NS * KK) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -266,12 +274,14 @@ __device__ __forceinline__ uint64_t finish(const F& f, u128 lo, u128 hi, uint64_
   }
 }
 
-template <class F, int LIMBS>
+template <class F, int LIMBS, int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
                        int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err) {
-  using SH = Shape<LIMBS>;
+  using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
+  constexpr int kStages = SH::STAGES;
+  constexpr int kCDepth = SH::CDEPTH;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sA = smem;                        // A_BYTES
   uint8_t* sB = smem + SH::A_BYTES;          // kStages * 8 KB
@@ -372,12 +382,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint8_t* bt = sB + st * SH::B_BYTES;
         const uint32_t dacc = tmem + ab * 256;
         if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
-          mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, 512), id_zero, 0);
+          mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, SH::SBO), id_zero, 0);
 #pragma unroll
         for (int i = 0; i < LIMBS; ++i)
 #pragma unroll
-          for (int ks = 0; ks < kK / 32; ++ks)
-            mma_i8(dacc + i * NS, smem_desc(sA + i * kTileBytes + ks * 256, 512), smem_desc(bt + ks * 256, 512),
+          for (int ks = 0; ks < KK / 32; ++ks)
+            mma_i8(dacc + i * NS, smem_desc(sA + i * SH::TILE + ks * 256, SH::SBO), smem_desc(bt + ks * 256, SH::SBO),
                    id_full, (i > 0 || ks > 0) ? 1u : 0u);
         mma_commit(b_empty + st);
         mma_commit(acc_full + ab);
@@ -625,23 +635,25 @@ int limbs_for(uint64_t p) {
   return bits <= 8 ? 1 : bits <= 16 ? 2 : bits <= 32 ? 4 : 8;
 }
 
-template <int LIMBS>
+template <int LIMBS, int KK>
 void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K, uint8_t* Aw, cudaStream_t st) {
   const int mpad = ((rend - rbeg + 127) / 128) * 128;
-  split_a_kernel<LIMBS><<<(mpad * 4 + 255) / 256, 256, 0, st>>>(A, lda, r0, rbeg, rend, K, mpad, Aw);
+  const int64_t threads = (int64_t)mpad * Shape<LIMBS, KK>::KC;
+  split_a_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(A, lda, r0, rbeg, rend, K, mpad, Aw);
 }
 
-template <int LIMBS>
+template <int LIMBS, int KK>
 void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw, cudaStream_t st) {
-  constexpr int NS = Shape<LIMBS>::NS;
+  constexpr int NS = Shape<LIMBS, KK>::NS;
   const int npad = ((cend - jend + NS - 1) / NS) * NS;
-  split_b_kernel<LIMBS><<<(npad * 4 + 255) / 256, 256, 0, st>>>(B, ldb, jend, cend, K, npad, Bw);
+  const int64_t threads = (int64_t)npad * Shape<LIMBS, KK>::KC;
+  split_b_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(B, ldb, jend, cend, K, npad, Bw);
 }
 
-template <class F, int LIMBS>
+template <class F, int LIMBS, int KK>
 void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint8_t* Aw,
               const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st) {
-  using SH = Shape<LIMBS>;
+  using SH = Shape<LIMBS, KK>;
   Sched S;
   S.mtiles = (rend - rbeg + 127) / 128;
   S.nsub = (cend - jend + SH::NS - 1) / SH::NS;
@@ -649,60 +661,72 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
   const int grid = total < max_ctas ? (int)total : max_ctas;  // one CTA per SM: it owns all 512 TMEM columns
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
+    cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
     attr = true;
   }
-  trailing_tc_kernel<F, LIMBS><<<grid, kThreads, SH::SMEM, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64, err);
+  trailing_tc_kernel<F, LIMBS, KK><<<grid, kThreads, SH::SMEM, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64,
+                                                                      err);
 }
+
+// (limb count, K tile) of a prime and an update depth.
+inline int limbs_of(uint64_t p) { return p == kM61 ? 8 : limbs_for(p); }
 
 }  // namespace tc
 
 int tc_crossover_n(uint64_t) { return 512; }
 
-size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc::kK * 8; }
-size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kK * 8; }
+// Calls OP(limbs, K tile) for fp.p and K, both compile-time constants.
+#define MODLIN_TC_DISPATCH(OP)                      \
+  do {                                              \
+    const bool k128 = K > 64;                       \
+    switch (tc::limbs_of(fp.p)) {                   \
+      case 1: k128 ? OP(1, 128) : OP(1, 64); break; \
+      case 2: k128 ? OP(2, 128) : OP(2, 64); break; \
+      case 4: k128 ? OP(4, 128) : OP(4, 64); break; \
+      default: k128 ? OP(8, 128) : OP(8, 64); break; \
+    }                                               \
+  } while (0)
+
+size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc::kKMax * 8; }
+size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kKMax * 8; }
 
 cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
                        uint8_t* Aw, cudaStream_t st) {
   if (rbeg >= rend) return cudaSuccess;
-  if (K <= 0 || K > tc::kK) return cudaErrorInvalidValue;
-  switch (fp.p == kM61 ? 8 : tc::limbs_for(fp.p)) {
-    case 1: tc::split_a_t<1>(A, lda, r0, rbeg, rend, K, Aw, st); break;
-    case 2: tc::split_a_t<2>(A, lda, r0, rbeg, rend, K, Aw, st); break;
-    case 4: tc::split_a_t<4>(A, lda, r0, rbeg, rend, K, Aw, st); break;
-    default: tc::split_a_t<8>(A, lda, r0, rbeg, rend, K, Aw, st); break;
-  }
+  if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
+#define MODLIN_SPLIT_A(LL, KK) tc::split_a_t<LL, KK>(A, lda, r0, rbeg, rend, K, Aw, st)
+  MODLIN_TC_DISPATCH(MODLIN_SPLIT_A);
+#undef MODLIN_SPLIT_A
   return cudaGetLastError();
 }
 
 cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
                        cudaStream_t st) {
   if (jend >= cend) return cudaSuccess;
-  if (K <= 0 || K > tc::kK) return cudaErrorInvalidValue;
-  switch (fp.p == kM61 ? 8 : tc::limbs_for(fp.p)) {
-    case 1: tc::split_b_t<1>(B, ldb, jend, cend, K, Bw, st); break;
-    case 2: tc::split_b_t<2>(B, ldb, jend, cend, K, Bw, st); break;
-    case 4: tc::split_b_t<4>(B, ldb, jend, cend, K, Bw, st); break;
-    default: tc::split_b_t<8>(B, ldb, jend, cend, K, Bw, st); break;
-  }
+  if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
+#define MODLIN_SPLIT_B(LL, KK) tc::split_b_t<LL, KK>(B, ldb, jend, cend, K, Bw, st)
+  MODLIN_TC_DISPATCH(MODLIN_SPLIT_B);
+#undef MODLIN_SPLIT_B
   return cudaGetLastError();
 }
 
-cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
                       const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st) {
   if (rbeg >= rend || jend >= cend) return cudaSuccess;
+  if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
   const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
   if (fp.p == kM61) {
-    tc::update_t<FpM61, 8>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
-  } else {
-    const FpBarrett f(fp);
-    switch (tc::limbs_for(fp.p)) {
-      case 1: tc::update_t<FpBarrett, 1>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
-      case 2: tc::update_t<FpBarrett, 2>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
-      case 4: tc::update_t<FpBarrett, 4>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
-      default: tc::update_t<FpBarrett, 8>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st); break;
-    }
+    if (K > 64)
+      tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
+    else
+      tc::update_t<FpM61, 8, 64>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
+    return cudaGetLastError();
   }
+  const FpBarrett f(fp);
+#define MODLIN_UPDATE(LL, KK) \
+  tc::update_t<FpBarrett, LL, KK>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st)
+  MODLIN_TC_DISPATCH(MODLIN_UPDATE);
+#undef MODLIN_UPDATE
   return cudaGetLastError();
 }
 
@@ -710,10 +734,10 @@ cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, i
                                const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
                                uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
   if (rbeg >= rend || jend >= cend || K <= 0) return cudaSuccess;
-  if (K > tc::kK) return cudaErrorInvalidValue;
+  if (K > tc::kKMax) return cudaErrorInvalidValue;
   cudaError_t e = tc_split_a(fp, Lbuf, lda, r0, rbeg, rend, K, Aw, st);
   if (e == cudaSuccess) e = tc_split_b(fp, Ubuf, ldU, jend, cend, K, Bw, st);
-  if (e == cudaSuccess) e = tc_update(fp, m, ld, rbeg, rend, jend, cend, Aw, Bw, num_sms, err, st);
+  if (e == cudaSuccess) e = tc_update(fp, m, ld, rbeg, rend, jend, cend, K, Aw, Bw, num_sms, err, st);
   return e;
 }
 

@@ -11,10 +11,10 @@ namespace modlin {
 
 // Smallest side for which MODLIN_RANK_AUTO uses the tensor-core update.
 int tc_crossover_n(uint64_t p);
-// Workspace bytes for the limb planes of L (rows x K) and U (K x cols).
+// Workspace bytes for the limb planes of L (rows x K) and U (K x cols), K <= 128.
 size_t tc_a_bytes(int rows);
 size_t tc_b_bytes(int cols);
-// A[rbeg..rend, jend..cend] -= L * U mod p via exact INT8-limb GEMMs (L row
+// A[rbeg..rend, jend..cend] -= L * U mod p, K <= 128, via exact INT8-limb GEMMs (L row
 // r at Lbuf[(r - r0) * lda], U row k at Ubuf[k * ldU], absolute columns). `err` points
 // at two device ints (zeroed by the caller); err[0] != 0 afterwards means a
 // bounded wait inside the kernel expired.
@@ -25,12 +25,13 @@ cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, i
 // The three steps of launch_trailing_tc, for callers that reuse one operand's
 // limb planes across launches: limb planes of A rows [rbeg, rend) (row r at
 // A[(r - r0) * lda]), of B columns [jend, cend) (row k at B[k * ldb]), and the
-// update A[rbeg..rend, jend..cend] -= A * B on at most max_ctas SMs.
+// update A[rbeg..rend, jend..cend] -= A * B on at most max_ctas SMs. The same
+// K (<= 64 or <= 128: two plane layouts) must be given to all three.
 cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
                        uint8_t* Aw, cudaStream_t st);
 cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
                        cudaStream_t st);
-cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
+cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
                       const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st);
 
 }  // namespace modlin

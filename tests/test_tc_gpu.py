@@ -19,7 +19,7 @@ def run(M, p, C, L, U, kernel):
     import torch
     Mr, N = C.shape
     K = U.shape[0]
-    Lp = np.zeros((Mr, 64), dtype=np.uint64)
+    Lp = np.zeros((Mr, 64 if K <= 64 else 128), dtype=np.uint64)
     Lp[:, :K] = L
     dC = torch.from_numpy(C.view(np.int64).copy()).cuda()
     dL = torch.from_numpy(Lp.view(np.int64).copy()).cuda()
@@ -64,3 +64,32 @@ def test_large_tc_equals_plain(M, p):
     for Mr, N, K in [(2048, 1536, 64), (1000, 3001, 17), (4096, 512, 64)]:
         C, L, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
         assert np.array_equal(run(M, p, C, L, U, "tc"), run(M, p, C, L, U, "plain")), (p, Mr, N, K)
+
+
+@pytest.mark.parametrize("p", PRIMES)
+def test_two_panel_depth_exact(M, p):
+    """K up to 128 (two panels per pass, 128-byte limb rows): exact, and the
+    largest sums (all entries p-1) still fit the 32-bit accumulators."""
+    rng = np.random.default_rng(p % 977)
+    for Mr, N, K in [(128, 16, 128), (300, 130, 128), (131, 45, 65), (257, 200, 100)]:
+        C, L, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
+        assert np.array_equal(run(M, p, C, L, U, "tc"), exact(p, C, L, U)), (p, Mr, N, K)
+    Mr, N, K = 129, 33, 128
+    C = np.full((Mr, N), p - 1, dtype=np.uint64)
+    L = np.full((Mr, K), p - 1, dtype=np.uint64)
+    U = np.full((K, N), p - 1, dtype=np.uint64)
+    got = run(M, p, C, L, U, "tc")
+    assert np.array_equal(got[:4, :4], exact(p, C[:4, :4], L[:4], U[:, :4]))
+    assert (got == got[0, 0]).all()
+
+
+def test_two_panel_depth_large(M):
+    """A K = 128 update equals two K = 64 updates in a row."""
+    rng = np.random.default_rng(11)
+    for p in [M61, 65521]:
+        Mr, N = 3000, 2500
+        C, L, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, 128)), rand_res(rng, p, (128, N))
+        one = run(M, p, C, L, U, "tc")
+        two = run(M, p, run(M, p, C, L[:, :64], U[:64], "tc"), L[:, 64:], U[64:], "tc")
+        assert np.array_equal(one, two)
+        assert np.array_equal(two, run(M, p, run(M, p, C, L[:, :64], U[:64], "plain"), L[:, 64:], U[64:], "plain"))
