@@ -147,9 +147,10 @@ def int8_peak_tops(torch):
         return None
 
 
-def cpu_rank_sample(threads=0, target_s=12.0):
+def cpu_rank_sample(threads=0, target_s=15.0):
     """The oracle's blocked rank (the reference algorithm, OpenMP over rows)
-    on a uniform matrix over 2^61-1 sized for ~10-30 s of CPU work."""
+    on a uniform matrix over 2^61-1, sized from a 1024^2 probe so that the
+    sample takes about target_s seconds of CPU time (10-30 s)."""
     import oracle
     n0 = 1024
     m = oracle.gen_uniform(M61, 7, n0 * n0)
@@ -157,9 +158,9 @@ def cpu_rank_sample(threads=0, target_s=12.0):
     r, pc = oracle.rank(M61, m, n0, threads=threads, with_pcols=True)
     dt = time.perf_counter() - t0
     rate = algorithmic_work(n0, pc) / dt
-    n = n0
-    while n < 8192 and algorithmic_work(2 * n, range(2 * n)) / rate < target_s:
-        n *= 2
+    # W(n) ~ n^3 / 3: the side whose predicted time is target_s, in steps of 64.
+    n = int((3 * rate * target_s) ** (1 / 3)) // 64 * 64
+    n = max(n0, min(n, 8192))
     if n != n0:
         m = oracle.gen_uniform(M61, 7, n * n)
         t0 = time.perf_counter()
@@ -479,7 +480,7 @@ def run_reference(args, rank, world):
     cores = host_cores()
     samples = []
     for i in range(args.warmup + args.steps):
-        s = cpu_rank_sample(threads=0, target_s=8.0)
+        s = cpu_rank_sample(threads=0, target_s=12.0)
         if i >= args.warmup:
             samples.append(s)
     v = statistics.median([s["value"] for s in samples])
@@ -579,6 +580,7 @@ def main():
     barrier()
     launches0 = modlin.kernel_launches()
     trailing_ms = []
+    trailing_macs = []
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier()
@@ -588,6 +590,7 @@ def main():
         for _ in range(args.steps):
             ranks.append(step(kernel))
             trailing_ms.append(modlin.last_trailing_ms())
+            trailing_macs.append(modlin.last_trailing_macs())
         ev1.record()
         torch.cuda.synchronize()
         barrier()
@@ -654,7 +657,11 @@ def main():
     if rank == 0:
         peaks = measured_peaks()
         tr_ms = statistics.median(trailing_ms)
-        n_tr = sum(1 for _ in range(0, n, 64)) - 1
+        Wtr = statistics.median(trailing_macs)
+        # Timed trailing updates per rank: one per two-panel step on the
+        # tensor-core path (K = 128), one per panel on the plain path.
+        depth = 128 if kernel == "tc" else 64
+        n_tr = sum(1 for _ in range(0, n, depth)) - 1
         per_launch_ms = tr_ms / max(n_tr, 1)
         if kernel == "tc":
             int8 = int8_peak_tops(torch)
@@ -667,7 +674,8 @@ def main():
             roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None, "kernel": "trailing_tc (tcgen05 kind::i8)",
                     "peak_source": peak_note,
-                    "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops",
+                    "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops "
+                                              f"(K = {depth}, {n_tr} updates per rank)",
                     "avg_launch_ms": per_launch_ms}
         else:
             peak = peaks.get("hbm_gbs", 6650.0)
@@ -684,7 +692,7 @@ def main():
                     "int_pipe_modmac_per_s": Wtr / (tr_ms * 1e-3)}
         cpu = None
         if not args.no_cpu_baseline:
-            s = cpu_rank_sample(threads=0, target_s=12.0)
+            s = cpu_rank_sample(threads=0, target_s=15.0)
             cpu = {"value": s["value"], "unit": UNIT, "cores": host_cores(), "kind": "port",
                    "sample": f"oracle rank (src/fp.rs:125-255 restated, OpenMP) of one uniform {s['n']}x{s['n']} "
                              f"matrix over 2^61-1, {s['seconds']:.1f} s, on {cpu_model()}"}

@@ -219,6 +219,9 @@ uint64_t modlin_kernel_launches(void);
 /* Milliseconds spent in the trailing-update kernels of the last rank call,
  * measured with CUDA events on the launching stream (0 if unavailable). */
 double modlin_last_trailing_ms(void);
+/* Modular multiply-adds done by those timed trailing updates (rows x columns
+ * x depth of each), so that their rate is this / the time above. */
+double modlin_last_trailing_macs(void);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

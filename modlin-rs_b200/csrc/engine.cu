@@ -24,6 +24,7 @@ namespace modlin {
 
 std::atomic<uint64_t> g_launches{0};
 static double g_last_trailing_ms = 0.0;
+static double g_last_trailing_macs = 0.0;
 
 // ---------------------------------------------------------------------------
 // Per-device context: one stream, cached workspaces, pinned staging.
@@ -196,8 +197,21 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   uint64_t* Vneg = nullptr;
   int* h_status = reinterpret_cast<int*>(C->h_out);
   int pre_status = -1;
+  // Two-panel steps (128 columns, K = 128 trailing update): blocks V11 = P11^-1
+  // (negated), Y = P21 V11, S = P22 - Y P12 and VS = S^-1 (negated), and the
+  // look-ahead result for the next two-panel step.
+  uint64_t *V11n = nullptr, *Yb = nullptr, *Sb = nullptr, *VSn = nullptr;
+  int pre128 = -1;
+  uint64_t* Hb = Lbuf;  // two-panel multipliers [H1 H2], row stride 128
+  const size_t blk = (size_t)kPanel * kPanel;
   if (tc) {
-    CK(C->binv.ensure(256 + (size_t)kPanel * kPanel * 8));
+    CK(C->binv.ensure(256 + 5 * blk * 8));
+    CK(C->lbuf.ensure((size_t)n * 2 * kPanel * 8));
+    Lbuf = Hb = C->lbuf.as<uint64_t>();
+    V11n = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256) + blk;
+    Yb = V11n + blk;
+    Sb = Yb + blk;
+    VSn = Sb + blk;
     CK(C->tcBn.ensure(tc_b_bytes(kPanel)));
     binv_status = C->binv.as<int>();
     Vneg = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
@@ -208,11 +222,117 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     }
   }
 
+  // Enqueue on `s` the four 64 x 64 blocks of the two-panel step at
+  // (rr, cc) and copy the status word `slot` (nonzero: P11 or S singular)
+  // to the host.
+  auto prep128 = [&](int rr, int cc, cudaStream_t s, int slot) -> cudaError_t {
+    cudaError_t e = cudaMemsetAsync(binv_status + slot, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const uint64_t* P11 = R.m + (int64_t)rr * ld + cc;
+    const uint64_t* P12 = P11 + kPanel;
+    const uint64_t* P21 = P11 + (int64_t)kPanel * ld;
+    const uint64_t* P22 = P21 + kPanel;
+    launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, binv_status + slot, s);
+    launch_small_gemm64<F>(f, P21, ld, V11n, kPanel, nullptr, 0, Yb, kPanel, true, s);  // Y = P21 V11
+    launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s);      // S = P22 - Y P12
+    launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, binv_status + slot, s);
+    g_launches += 5;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(h_status + slot, binv_status + slot, sizeof(int), cudaMemcpyDeviceToHost, s);
+  };
+  double trailing_macs = 0;
+
   int rank = 0, col = 0;
   while (col < n && rank < n) {
     const int jend = std::min(col + kPanel, n);
     const int W = jend - col;
     const int r0 = rank;
+    if (tc && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
+      // Two-panel block step: P = A[r0 .. r0+128, col .. col+128) split into
+      // 64 x 64 blocks [P11 P12; P21 P22]. With V11 = P11^-1 and the Schur
+      // complement S = P22 - P21 V11 P12 invertible, the multipliers of the
+      // rows below, H = X_P P^-1 = [H1 H2], come from four n x 64 x 64
+      // products,
+      //   G1 = X1 V11,  X2' = X2 - G1 P12,  H2 = X2' S^-1,  H1 = G1 - H2 Y,
+      // (Y = P21 V11), and the trailing block takes one K = 128 update
+      // A[r0+128.., col+128..] -= H * A[r0 .. r0+128, col+128..]: half the
+      // epilogue work per modMAC of two one-panel updates.
+      int status = pre128;
+      pre128 = -1;
+      if (status < 0) {
+        CK(prep128(r0, col, st, 0));
+        CK(cudaStreamSynchronize(st));
+        status = h_status[0];
+      }
+      if (status == 0) {
+        pre_status = -1;
+        const int c2 = col + 2 * kPanel;
+        const int rb = r0 + 2 * kPanel;
+        const int rows = n - rb;
+        uint8_t* tA = C->tcA.as<uint8_t>();
+        uint8_t* tB = C->tcB.as<uint8_t>();
+        int* terr = C->tcerr.as<int>();
+        if (rows > 0) {
+          CK(cudaMemsetAsync(Hb + (size_t)2 * kPanel * 2 * kPanel, 0, (size_t)rows * 2 * kPanel * 8, st));
+          const int64_t H0 = 2 * kPanel;  // H rows relative to r0, stride 128
+          const uint64_t* X1 = R.m + (int64_t)r0 * ld + col;
+          // G1 = X1 V11 into H[:, 0:64).
+          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, kPanel, X1, ld, 0, V11n, kPanel, kPanel, tA, tB,
+                                C->num_sms, terr, st));
+          // X2 -= G1 P12 (rows below the block, in place).
+          CK(launch_trailing_tc(*R.fp, R.m, ld, rb, n, col + kPanel, c2, Hb, H0, r0, R.m + (int64_t)r0 * ld, ld,
+                                kPanel, tA, tB, C->num_sms, terr, st));
+          // H2 = X2' S^-1 into H[:, 64:128).
+          CK(launch_trailing_tc(*R.fp, Hb + kPanel, H0, 2 * kPanel, n - r0, 0, kPanel, X1 + kPanel, ld, 0, VSn, kPanel,
+                                kPanel, tA, tB, C->num_sms, terr, st));
+          // H1 = G1 - H2 Y.
+          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, kPanel, Hb + kPanel, H0, 0, Yb, kPanel, kPanel,
+                                tA, tB, C->num_sms, terr, st));
+          g_launches += 13;
+          if (c2 < n) {
+            const uint64_t* Ub = R.m + (int64_t)r0 * ld;  // the 128 pivot rows, as they are
+            auto evp = take_events();
+            cudaEventRecord(evp.first, st);
+            CK(tc_split_a(*R.fp, Hb, H0, r0, rb, n, 2 * kPanel, tA, st));
+            const bool ahead = c2 + 2 * kPanel <= n && n - rb >= 2 * kPanel;
+            int cw = c2;
+            if (ahead) {
+              // The next step's 128 columns first; its blocks on the second
+              // stream while the rest updates.
+              CK(tc_split_b(*R.fp, Ub, ld, c2, c2 + 2 * kPanel, 2 * kPanel, C->tcBn.as<uint8_t>(), st));
+              CK(tc_update(*R.fp, R.m, ld, rb, n, c2, c2 + 2 * kPanel, 2 * kPanel, tA, C->tcBn.as<uint8_t>(),
+                           C->num_sms, terr, st));
+              CK(cudaEventRecord(C->ev_narrow, st));
+              CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
+              CK(prep128(rb, c2, C->aux, 1));
+              CK(cudaEventRecord(C->ev_inv, C->aux));
+              g_launches += 2;
+              cw = c2 + 2 * kPanel;
+            }
+            if (cw < n) {
+              CK(tc_split_b(*R.fp, Ub, ld, cw, n, 2 * kPanel, tB, st));
+              CK(tc_update(*R.fp, R.m, ld, rb, n, cw, n, 2 * kPanel, tA, tB, ahead ? C->num_sms - 1 : C->num_sms,
+                           terr, st));
+              g_launches += 2;
+            }
+            cudaEventRecord(evp.second, st);
+            g_launches += 1;
+            trailing_macs += (double)rows * (n - c2) * (2 * kPanel);
+            if (ahead) {
+              CK(cudaEventSynchronize(C->ev_inv));
+              pre128 = h_status[1];
+            }
+          }
+        }
+        if (R.pcols)
+          for (int k = 0; k < 2 * kPanel; ++k) R.pcols->push_back(col + k);
+        rank += 2 * kPanel;
+        col = c2;
+        if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
+        continue;
+      }
+    }
     if (tc && W == kPanel && n - r0 >= kPanel) {
       // Block step. When the diagonal block P = A[r0 .. r0+64, col .. jend) is
       // invertible, its rows are this panel's pivot rows and col .. jend its
@@ -275,6 +395,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
             }
             cudaEventRecord(evp.second, st);
             g_launches += 1;
+            trailing_macs += (double)rows * (n - jend) * kPanel;
             if (ahead) {
               CK(cudaEventSynchronize(C->ev_inv));
               pre_status = h_status[1];
@@ -334,6 +455,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       }
       auto evp = take_events();
       cudaEventRecord(evp.first, st);
+      trailing_macs += (double)(n - r0 - pb) * (n - jend) * pb;
       if (tc) {
         CK(launch_trailing_tc(*R.fp, R.m, ld, r0 + pb, n, jend, n, Lbuf, kPanel, r0, Ubuf, n, pb, C->tcA.as<uint8_t>(),
                               C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
@@ -365,6 +487,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     if (cudaEventElapsedTime(&ms, C->ev[2 * i], C->ev[2 * i + 1]) == cudaSuccess) tms += ms;
   }
   g_last_trailing_ms = tms;
+  g_last_trailing_macs = trailing_macs;
   *rank_out = (size_t)rank;
   return MODLIN_OK;
 }
@@ -983,5 +1106,7 @@ int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) 
 uint64_t modlin_kernel_launches(void) { return g_launches.load(); }
 
 double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
+
+double modlin_last_trailing_macs(void) { return g_last_trailing_macs; }
 
 }  // extern "C"

@@ -400,6 +400,48 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 }
 
 // ---------------------------------------------------------------------------
+// small_gemm64_kernel — one CTA of 1024 threads: C = D - A * B (negate) or
+// C = D + A * B on 64 x 64 blocks mod p (D may be null: zero), operands
+// staged in shared memory, one reduction per output.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(kInvThreads) small_gemm64_kernel(F f, const uint64_t* __restrict__ A, int64_t lda,
+                                                                    const uint64_t* __restrict__ B, int64_t ldb,
+                                                                    const uint64_t* __restrict__ D, int64_t ldd,
+                                                                    uint64_t* __restrict__ Cout, int64_t ldc,
+                                                                    int negate) {
+  extern __shared__ __align__(16) uint64_t smem_g[];
+  uint64_t(*As)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_g);
+  uint64_t(*Bs)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_g + kPanel * (kPanel + 1));
+  const int tid = threadIdx.x, i = tid >> 4, s = tid & 15;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = s + 16 * q;
+    As[i][j] = A[(int64_t)i * lda + j];
+    Bs[i][j] = B[(int64_t)i * ldb + j];
+  }
+  __syncthreads();
+  const uint64_t p = f.modulus(), sb = f.safe_batch();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = s + 16 * q;
+    u128 acc = 0;
+    uint64_t cnt = 0;
+    for (int k = 0; k < kPanel; ++k) {
+      acc += f.prod(As[i][k], Bs[k][j]);
+      if (++cnt == sb) {
+        acc = f.reduce(acc);  // counts as one product from here on
+        cnt = 1;
+      }
+    }
+    uint64_t v = f.reduce(acc);
+    if (negate && v) v = p - v;
+    if (D) v = f.add(v, D[(int64_t)i * ldd + j]);
+    Cout[(int64_t)i * ldc + j] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Launch wrappers (explicit instantiation for both field policies).
 // ---------------------------------------------------------------------------
 template <class F>
@@ -473,7 +515,21 @@ void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int
   block_inverse_kernel<F><<<1, kInvThreads, smem, st>>>(f, m, ld, r0, col, Vneg, status);
 }
 
+template <class F>
+void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
+                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st) {
+  const size_t smem = 2 * kPanel * (kPanel + 1) * sizeof(uint64_t);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(small_gemm64_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  small_gemm64_kernel<F><<<1, kInvThreads, smem, st>>>(f, A, lda, B, ldb, D, ldd, C, ldc, negate ? 1 : 0);
+}
+
 #define INSTANTIATE(F)                                                                                          \
+  template void launch_small_gemm64<F>(const F&, const uint64_t*, int64_t, const uint64_t*, int64_t,            \
+                                       const uint64_t*, int64_t, uint64_t*, int64_t, bool, cudaStream_t);       \
   template void launch_block_inverse<F>(const F&, const uint64_t*, int64_t, int, int, uint64_t*, int*,          \
                                         cudaStream_t);                                                          \
   template void launch_window<F>(const F&, const uint64_t*, int64_t, int, int, int, int, int, PanelState*,       \

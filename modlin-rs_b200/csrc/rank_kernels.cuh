@@ -14,6 +14,10 @@ namespace modlin {
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
                           cudaStream_t st);
+// C = D - A * B (negate) or D + A * B on 64 x 64 blocks (D may be null).
+template <class F>
+void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
+                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st);
 template <class F>
 void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
                    PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,

@@ -32,3 +32,8 @@ def kernel_launches() -> int:
 def last_trailing_ms() -> float:
     """CUDA-event time of the last rank call's trailing-update kernels."""
     return float(lib().modlin_last_trailing_ms())
+
+
+def last_trailing_macs() -> float:
+    """Modular multiply-adds done by those timed trailing updates."""
+    return float(lib().modlin_last_trailing_macs())
