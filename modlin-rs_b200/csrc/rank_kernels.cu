@@ -327,10 +327,19 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
 }
 
 // ---------------------------------------------------------------------------
-// block_inverse_kernel — one CTA of 1024 threads: the inverse of the 64 x 64
-// block P = A[r0 .. r0+64, col .. col+64) by fraction-free Gauss-Jordan on
-// [P | I] in shared memory (row j <- e * row j - h * pivot row, one reduction
-// of the two-product sum per entry), or status = 1 when P is singular.
+// block_inverse_kernel — one CTA of 1024 threads (16 per block row): the
+// inverse of the 64 x 64 block P = A[r0 .. r0+64, col .. col+64), or
+// status = 1 when P is singular. In-place fraction-free Gauss-Jordan: at
+// column c with pivot row `piv` (the first row not yet used whose entry is
+// nonzero) every other row j becomes e * row_j - h * row_piv (e = P[piv][c],
+// h = P[j][c]: one reduction of the two-product sum per entry), and column c,
+// now zero outside the pivot, stores column `piv` of the accumulated row
+// operations E instead (-h s and s in the pivot row, s = the scale row piv
+// took while it was not a pivot). Row j's remaining left entry d_j is tracked
+// apart. At the end P^-1 [pc_j][i] = E[j][i] / d_j with
+// E[j][i] stored at column pc_i. One block barrier per column: the owner of
+// column c+1 in each row flags a nonzero entry before it, and every warp then
+// finds the pivot by itself with a ballot over the flags.
 // Output: Vneg[c][i] = -(P^-1)[c][i] (row c = panel column, column i =
 // block row), the B operand of the multiplier GEMM H = X_P * P^-1.
 // ---------------------------------------------------------------------------
@@ -339,63 +348,77 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
                                                                      int32_t r0, int32_t col,
                                                                      uint64_t* __restrict__ Vneg, int* status) {
   extern __shared__ __align__(16) uint64_t smem_inv[];
-  uint64_t(*A)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv);
-  uint64_t(*B)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv + kPanel * (kPanel + 1));
-  __shared__ uint64_t d[kPanel], dinv[kPanel];
-  __shared__ int32_t used[kPanel], pc[kPanel];
-  __shared__ int32_t sh_piv;
+  uint64_t(*M)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv);
+  __shared__ uint64_t d[kPanel], dinv[kPanel], sc[kPanel];
+  __shared__ int32_t pc[kPanel];
+  __shared__ uint8_t nz[2][kPanel];  // nz[c & 1][j]: row j's entry in column c is nonzero
   const uint64_t p = f.modulus();
   const int tid = threadIdx.x, j = tid >> 4, s = tid & 15;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int c = s + 16 * q;
-    A[j][c] = m[(int64_t)(r0 + j) * ld + col + c];
-    B[j][c] = j == c;
-  }
+  for (int q = 0; q < 4; ++q) M[j][s + 16 * q] = m[(int64_t)(r0 + j) * ld + col + s + 16 * q];
   if (s == 0) {
-    used[j] = 0;
     d[j] = 0;
+    sc[j] = 1;
+    nz[0][j] = M[j][0] != 0;  // written by this thread just above
   }
   __syncthreads();
+  const int lane = tid & 31;
+  unsigned long long used = 0;  // rows that are pivots already (same in every thread)
+  int last_piv = -1;     // the previous column's pivot row: its column gets E's entry now
+  uint64_t last_sc = 0;  // that entry: the pivot row's scale
   for (int c = 0; c < kPanel; ++c) {
-    if (tid < 32) {
-      const bool lo = !used[tid] && A[tid][c] != 0, hi = !used[tid + 32] && A[tid + 32][c] != 0;
-      const uint32_t b0 = __ballot_sync(0xffffffffu, lo), b1 = __ballot_sync(0xffffffffu, hi);
-      if (tid == 0) sh_piv = b0 ? __ffs(b0) - 1 : (b1 ? 31 + __ffs(b1) : -1);
-    }
-    __syncthreads();
-    const int piv = sh_piv;
-    if (piv < 0) {
+    // Deferred from the previous column, after every thread has read the
+    // pivot value there; only this thread reads this entry before the next
+    // barrier.
+    if (j == last_piv && s == ((c - 1) & 15)) M[j][c - 1] = last_sc;
+    // Every warp finds the pivot itself: the first row not yet used with a
+    // nonzero entry in column c (a ballot over the 64 rows' flags, set before
+    // the barrier by the thread that owns column c of each row).
+    const bool lo = !((used >> lane) & 1) && nz[c & 1][lane];
+    const bool hi = !((used >> (lane + 32)) & 1) && nz[c & 1][lane + 32];
+    const uint32_t b0 = __ballot_sync(0xffffffffu, lo), b1 = __ballot_sync(0xffffffffu, hi);
+    if ((b0 | b1) == 0) {  // no pivot in column c: P is singular
       if (tid == 0) *status = 1;
       return;
     }
-    const uint64_t e = A[piv][c];
-    const uint64_t h = j != piv ? A[j][c] : 0;
+    const int piv = b0 ? __ffs(b0) - 1 : 31 + __ffs(b1);
+    const uint64_t e = M[piv][c];
+    const uint64_t spiv = sc[piv];  // E[piv][piv]: the scale row piv took while unused
+    const uint64_t h = j != piv ? M[j][c] : 0;
+    __syncwarp();  // every read of M[j][c] precedes its overwrite below
     if (h != 0) {
       const uint64_t nh = p - h;
-      for (int cc = c + 1 + s; cc < kPanel; cc += 16) A[j][cc] = f.reduce(f.prod(e, A[j][cc]) + f.prod(nh, A[piv][cc]));
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int k = s + 16 * q;
-        const uint64_t bp = B[piv][k], bj = B[j][k];
-        if (bp | bj) B[j][k] = f.reduce(f.prod(e, bj) + f.prod(nh, bp));
+        M[j][k] = k == c ? f.mul(nh, spiv) : f.reduce(f.prod(e, M[j][k]) + f.prod(nh, M[piv][k]));
       }
-      if (s == 0 && used[j]) d[j] = f.mul(e, d[j]);
+      if (s == 0) {
+        if ((used >> j) & 1)
+          d[j] = f.mul(e, d[j]);
+        else
+          sc[j] = f.mul(e, sc[j]);
+      }
     }
     if (j == piv && s == 0) {
-      used[j] = 1;
-      pc[j] = c;
       d[j] = e;
+      pc[j] = c;
     }
+    const int cn = c + 1;
+    if (cn < kPanel && s == (cn & 15)) nz[cn & 1][j] = M[j][cn] != 0;
+    last_piv = piv;
+    last_sc = spiv;
+    used |= 1ULL << piv;
     __syncthreads();
   }
+  if (j == last_piv && s == ((kPanel - 1) & 15)) M[j][kPanel - 1] = last_sc;
   if (tid < kPanel) dinv[tid] = fp_inv_binary(d[tid], p);
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int k = s + 16 * q;
-    const uint64_t v = f.mul(B[j][k], dinv[j]);
-    Vneg[(int64_t)pc[j] * kPanel + k] = v ? p - v : 0;
+    const int i = s + 16 * q;
+    const uint64_t v = f.mul(M[j][pc[i]], dinv[j]);
+    Vneg[(int64_t)pc[j] * kPanel + i] = v ? p - v : 0;
   }
 }
 
@@ -506,7 +529,7 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int re
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
                           cudaStream_t st) {
-  const size_t smem = 2 * kPanel * (kPanel + 1) * sizeof(uint64_t);
+  const size_t smem = kPanel * (kPanel + 1) * sizeof(uint64_t);
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(block_inverse_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
