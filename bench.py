@@ -249,19 +249,24 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
         else:
             modlin.gen.uniform_device(M61, seed, t.data_ptr(), long_n)
         torch.cuda.synchronize()
-        for _ in range(warmup):
-            lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel="grid")
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel="grid")
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        res[name] = {"n": long_n, "lc": lc, "expected": long_L if planted else "about n/2", "ms": ms,
-                     "steps_per_s": long_n / (ms * 1e-3)}
-        if planted:
-            assert lc == long_L, (lc, long_L)
+        entry = {"n": long_n, "expected": long_L if planted else "about n/2"}
+        # The default (one 16-CTA cluster) and the whole-grid kernel.
+        for kern in ("cluster", "grid"):
+            for _ in range(warmup):
+                lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel=kern)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                lc = mfp.linear_complexity_device(M61, t.data_ptr(), long_n, kernel=kern)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            if planted:
+                assert lc == long_L, (lc, long_L)
+            entry["lc"] = lc
+            entry[kern] = {"ms": ms, "steps_per_s": long_n / (ms * 1e-3), "us_per_step": 1e3 * ms / long_n}
+        entry["steps_per_s"] = entry["cluster"]["steps_per_s"]
+        res[name] = entry
         del t
     jobs, iid_seeds = bm_batch_jobs(batch_count)
     arena, ptrs = bm_batch_build(torch, modlin, jobs, iid_seeds)

@@ -108,9 +108,11 @@ int modlin_trailing_update_device(uint64_t p, uint64_t *d_C, size_t ldc, size_t 
 
 /* ---- Linear complexity (src/fp.rs:257-308) ------------------------------ */
 
-#define MODLIN_LC_AUTO 0      /* block kernel for short, cooperative grid for long */
+#define MODLIN_LC_AUTO 0      /* block kernel for short, cluster for long, grid beyond the cluster */
 #define MODLIN_LC_BLOCK 1     /* one CTA runs the whole sequence (plain form) */
 #define MODLIN_LC_GRID 2      /* persistent cooperative kernel, one grid barrier per step */
+#define MODLIN_LC_CLUSTER 3   /* one 16-CTA thread-block cluster, one cluster barrier per step
+                                 (n <= 409600; MODLIN_EINVAL_N beyond) */
 
 typedef struct {
     int kernel;       /* MODLIN_LC_* */

@@ -36,7 +36,7 @@ __device__ __forceinline__ uint64_t partial_dot(const F& f, const uint64_t* c, c
   u128 acc = 0;
   uint64_t tot = 0, cnt = 0;
   for (int64_t j = jbeg; j <= jend_incl; j += stride) {
-    acc += (u128)c[j] * s[i - j];
+    acc += f.prod(c[j], s[i - j]);
     if (++cnt == sb) {
       tot = f.add(tot, f.reduce(acc));
       acc = 0;
@@ -78,13 +78,14 @@ __device__ int64_t bm_block_run(const F& f, const uint64_t* __restrict__ s, int6
       continue;
     }
     const bool lenchg = 2 * l <= i;
+    const uint64_t nd = f.modulus() - d;  // c <- bb c + (p - d) x^m b: one reduction per entry
     int64_t hi = l + 1 > m + bl ? l + 1 : m + bl;
     if (hi > n) hi = n;
     for (int64_t j = tid; j < hi; j += T) {
       const uint64_t old = c[j];
       const int64_t jb = j - m;
       const uint64_t bj = (jb >= 0 && jb < bl) ? b[jb] : 0;
-      c[j] = f.sub(f.mul(bb, old), f.mul(d, bj));
+      c[j] = f.reduce(f.prod(bb, old) + f.prod(nd, bj));
       if (lenchg && j <= l) t[j] = old;
     }
     if (lenchg) {
@@ -98,7 +99,10 @@ __device__ int64_t bm_block_run(const F& f, const uint64_t* __restrict__ s, int6
     } else {
       ++m;
     }
-    __syncthreads();
+    // No barrier here: every thread reads and writes only its own entries of
+    // c (j = tid mod T), ws is double-buffered, and the b entries written at
+    // a length change are first read after the next step's barrier, which
+    // every thread reaches only after finishing this step.
   }
   return l;
 }
@@ -117,8 +121,9 @@ __global__ void bm_block_kernel(BmJob job, uint64_t* gws, int64_t smem_words, in
   __shared__ uint64_t ws[2][32];
   uint64_t* base = (3 * job.n <= smem_words) ? bm_smem : gws;
   uint64_t *c = base, *b = base + job.n, *t = base + 2 * job.n;
-  const int64_t l = job.p == kM61 ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
-                                  : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
+  const int64_t l = job.p == kM61              ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
+                    : job.p < (1ULL << 32) ? bm_block_dispatch<FpSmall>(job, c, b, t, ws)
+                                           : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
   if (threadIdx.x == 0) *out = l;
 }
 
@@ -139,8 +144,9 @@ __global__ void bm_batch_kernel(const BmJob* __restrict__ jobs, int64_t count, u
     const BmJob job = jobs[q];
     uint64_t* base = (3 * job.n <= smem_words) ? bm_smem : gws + (int64_t)blockIdx.x * gws_words;
     uint64_t *c = base, *b = base + job.n, *t = base + 2 * job.n;
-    const int64_t l = job.p == kM61 ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
-                                    : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
+    const int64_t l = job.p == kM61              ? bm_block_dispatch<FpM61>(job, c, b, t, ws)
+                      : job.p < (1ULL << 32) ? bm_block_dispatch<FpSmall>(job, c, b, t, ws)
+                                             : bm_block_dispatch<FpBarrett>(job, c, b, t, ws);
     if (threadIdx.x == 0) out[job.slot] = l;
     __syncthreads();
   }
@@ -253,6 +259,7 @@ __global__ void bm_grid_kernel(F f, const uint64_t* __restrict__ s, int64_t n, i
       continue;
     }
     const bool lenchg = 2 * l <= i;
+    const uint64_t nd = f.modulus() - d;  // c <- bb c + (p - d) x^m b: one reduction per entry
     int64_t uhi = l + 1 > m + bl ? l + 1 : m + bl;
     if (uhi > n) uhi = n;
     const int64_t jhi = uhi < hi_own ? uhi : hi_own;
@@ -260,7 +267,7 @@ __global__ void bm_grid_kernel(F f, const uint64_t* __restrict__ s, int64_t n, i
       const uint64_t old = cs[j - lo];
       const int64_t jb = j - m;
       const uint64_t bj = (jb >= 0 && jb < bl) ? __ldcg(bcur + jb) : 0;
-      cs[j - lo] = f.sub(f.mul(bb, old), f.mul(d, bj));
+      cs[j - lo] = f.reduce(f.prod(bb, old) + f.prod(nd, bj));
       if (lenchg && j <= l) __stcg(bnext + j, old);
     }
     if (lenchg) {
@@ -279,6 +286,137 @@ __global__ void bm_grid_kernel(F f, const uint64_t* __restrict__ s, int64_t n, i
     __syncthreads();
   }
   if (blockIdx.x == 0 && tid == 0) *out = l;
+}
+
+// ---------------------------------------------------------------------------
+// Cluster kernel for one long sequence: one thread-block cluster (up to 16
+// CTAs of 512 threads on 16 SMs), each CTA owning a slice of c in shared
+// memory. The per-step all-reduce of the partial discrepancies is one
+// hardware cluster barrier: every CTA posts its partial in its own shared
+// memory, and after the barrier every warp reads the cluster's partials
+// through distributed shared memory. b lives in global memory (L2); its
+// writes before a barrier are visible to the whole cluster after it.
+// ---------------------------------------------------------------------------
+constexpr int kClusterMax = 16;  // CTAs per cluster (non-portable size)
+constexpr int kTileBatch = 8;    // tiles whose global loads are issued together
+constexpr int kClusterThreads = 512;  // threads per CTA = indices per tile
+
+template <class F>
+__global__ void __launch_bounds__(kClusterThreads, 1) bm_cluster_kernel(F f, const uint64_t* __restrict__ s, int64_t n,
+                                                             int64_t chunk, uint64_t* bbuf0, uint64_t* bbuf1,
+                                                             int64_t* out) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  // c is dealt out in tiles of TH = 512 consecutive indices, tile t to CTA
+  // t mod R (so the active prefix j <= l is spread over the whole cluster);
+  // thread tid owns index j = TH t + tid of each of its tiles.
+  constexpr int TH = kClusterThreads;
+  extern __shared__ __align__(16) uint64_t cs[];  // my tiles, TH words each
+  __shared__ uint64_t ws[TH / 32];
+  __shared__ uint64_t part[2][kClusterMax];  // [step parity][CTA]: partials pushed by every CTA
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int R = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int64_t ntiles = (n + TH - 1) / TH;
+  const int my_tiles = ntiles > rank ? (int)((ntiles - rank + R - 1) / R) : 0;
+  for (int k = 0; k < my_tiles; ++k) {
+    const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+    cs[(k * TH) + tid] = j == 0;
+    if (j < n) bbuf0[j] = j == 0;
+  }
+  uint64_t* part_dst = lane < R ? cl.map_shared_rank(&part[0][rank], lane) : nullptr;
+  cl.sync();
+  const uint64_t sb = f.safe_batch();
+  uint64_t* bcur = bbuf0;
+  uint64_t* bnext = bbuf1;
+  int64_t l = 0, m = 1, bl = 1;
+  uint64_t bb = 1;
+  for (int64_t i = 0; i < n; ++i) {
+    // Partial discrepancy over my indices j <= l; the loads of a batch of
+    // tiles are issued together so that one L2 latency covers them.
+    uint64_t tot = 0;
+    const int kend = (int)(l < 0 ? 0 : ((l / TH) - rank + R) / R);  // tiles that may hold j <= l
+    const int kn = kend < my_tiles ? kend : my_tiles;
+    for (int k0 = 0; k0 < kn; k0 += kTileBatch) {
+      uint64_t sv[kTileBatch], cv[kTileBatch];
+#pragma unroll
+      for (int q = 0; q < kTileBatch; ++q) {
+        const int k = k0 + q;
+        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+        const bool on = k < kn && j <= l;
+        sv[q] = on ? s[i - j] : 0;
+        cv[q] = on ? cs[(k * TH) + tid] : 0;
+      }
+      // Two independent chains of kTileBatch / 2 <= 4 <= safe_batch
+      // products each (p < 2^63), reduced at the end of the batch.
+      u128 a0 = 0, a1 = 0;
+#pragma unroll
+      for (int q = 0; q < kTileBatch; q += 2) {
+        a0 += f.prod(cv[q], sv[q]);
+        a1 += f.prod(cv[q + 1], sv[q + 1]);
+      }
+      tot = f.add(tot, f.add(f.reduce(a0), f.reduce(a1)));
+    }
+    uint64_t v = warp_sum_mod(f, tot);
+    if (lane == 0) ws[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      v = warp_sum_mod(f, lane < TH / 32 ? ws[lane] : 0);
+      v = __shfl_sync(0xffffffffu, v, 0);
+      // Push this CTA's partial into every CTA's shared memory.
+      if (lane < R) part_dst[(i & 1) * kClusterMax] = v;
+    }
+    cl.sync();
+    // Every warp sums the cluster's partials from its own shared memory
+    // (exact, so every thread gets the same discrepancy).
+    uint64_t dv = lane < R ? part[i & 1][lane] : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dv = f.add(dv, __shfl_xor_sync(0xffffffffu, dv, off));
+    const uint64_t d = dv;
+    if (d == 0) {
+      ++m;
+      continue;
+    }
+    const bool lenchg = 2 * l <= i;
+    const uint64_t nd = f.modulus() - d;  // c <- bb c + (p - d) x^m b: one reduction per entry
+    int64_t uhi = l + 1 > m + bl ? l + 1 : m + bl;
+    if (uhi > n) uhi = n;
+    const int kuend = (int)(((uhi - 1) / TH) - rank + R) / R;  // tiles that may hold j < uhi
+    const int ku = kuend < my_tiles ? kuend : my_tiles;
+    for (int k0 = 0; k0 < ku; k0 += kTileBatch) {
+      uint64_t bv[kTileBatch];
+#pragma unroll
+      for (int q = 0; q < kTileBatch; ++q) {
+        const int k = k0 + q;
+        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+        const int64_t jb = j - m;
+        bv[q] = (k < ku && j < uhi && jb >= 0 && jb < bl) ? __ldcg(bcur + jb) : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < kTileBatch; ++q) {
+        const int k = k0 + q;
+        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+        if (k < ku && j < uhi) {
+          uint64_t* cp = cs + (k * TH) + tid;
+          const uint64_t old = *cp;
+          *cp = f.reduce(f.prod(bb, old) + f.prod(nd, bv[q]));
+          if (lenchg && j <= l) __stcg(bnext + j, old);
+        }
+      }
+    }
+    if (lenchg) {
+      uint64_t* tmp = bcur;
+      bcur = bnext;
+      bnext = tmp;
+      bl = l + 1;
+      bb = d;
+      l = i + 1 - l;
+      m = 1;
+    } else {
+      ++m;
+    }
+  }
+  if (rank == 0 && tid == 0) *out = l;
+  cl.sync();  // no CTA leaves while others may still write into its shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -341,6 +479,61 @@ cudaError_t launch_bm_grid(const FieldParams& fp, const uint64_t* s, int64_t n, 
                            int* ctas_used) {
   if (fp.p == kM61) return launch_grid_t(FpM61(fp), s, n, ctas, threads, b0, b1, gs, spin, d_out, st, ctas_used);
   return launch_grid_t(FpBarrett(fp), s, n, ctas, threads, b0, b1, gs, spin, d_out, st, ctas_used);
+}
+
+template <class F>
+static cudaError_t launch_cluster_t(const F& f, const uint64_t* s, int64_t n, int R, uint64_t* b0, uint64_t* b1,
+                                   int64_t* d_out, cudaStream_t st) {
+  const int64_t ntiles = (n + kClusterThreads - 1) / kClusterThreads;
+  const int64_t chunk = (ntiles + R - 1) / R * kClusterThreads;  // words of c per CTA
+  const size_t smem = (size_t)chunk * 8;
+  cudaError_t e = cudaFuncSetAttribute(bm_cluster_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (R > 8) {
+    e = cudaFuncSetAttribute(bm_cluster_kernel<F>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(R);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = R;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  e = cudaOccupancyMaxActiveClusters(&nclusters, bm_cluster_kernel<F>, &cfg);
+  if (e != cudaSuccess) return e;
+  if (nclusters < 1) return cudaErrorInvalidConfiguration;
+  return cudaLaunchKernelEx(&cfg, bm_cluster_kernel<F>, f, s, n, chunk, b0, b1, d_out);
+}
+
+int bm_cluster_size(int64_t n) {
+  return ((n + kClusterThreads - 1) / kClusterThreads + 15) / 16 * kClusterThreads * 8 <= kBmClusterSliceBytes ? 16 : 0;
+}
+
+template <class F>
+static cudaError_t launch_cluster_any(const F& f, const uint64_t* s, int64_t n, int R, uint64_t* b0, uint64_t* b1,
+                                     int64_t* d_out, cudaStream_t st) {
+  cudaError_t e = launch_cluster_t(f, s, n, R, b0, b1, d_out, st);
+  // A device without 16-CTA clusters: 8 CTAs when the slices still fit.
+  if (e != cudaSuccess && R > 8 &&
+      ((n + kClusterThreads - 1) / kClusterThreads + 7) / 8 * kClusterThreads * 8 <= kBmClusterSliceBytes) {
+    cudaGetLastError();
+    e = launch_cluster_t(f, s, n, 8, b0, b1, d_out, st);
+  }
+  return e;
+}
+
+cudaError_t launch_bm_cluster(const FieldParams& fp, const uint64_t* s, int64_t n, int R, uint64_t* b0, uint64_t* b1,
+                              int64_t* d_out, cudaStream_t st) {
+  if (fp.p == kM61) return launch_cluster_any(FpM61(fp), s, n, R, b0, b1, d_out, st);
+  if (fp.p < (1ULL << 32)) return launch_cluster_any(FpSmall(fp), s, n, R, b0, b1, d_out, st);
+  return launch_cluster_any(FpBarrett(fp), s, n, R, b0, b1, d_out, st);
 }
 
 size_t grid_sync_bytes() { return sizeof(GridSync); }

@@ -26,6 +26,13 @@ int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words);
 cudaError_t launch_bm_grid(const FieldParams& fp, const uint64_t* s, int64_t n, int ctas, int threads, uint64_t* b0,
                            uint64_t* b1, void* gs, long long spin, int64_t* d_out, cudaStream_t st,
                            int* ctas_used);
+// One long sequence on one thread-block cluster of R = 16 CTAs (8 where 16
+// cannot be launched and the slices fit); b0, b1: n-word global workspaces.
+// bm_cluster_size gives R for n (0: too long for the cluster's shared memory).
+constexpr int64_t kBmClusterSliceBytes = 200 * 1024;
+int bm_cluster_size(int64_t n);
+cudaError_t launch_bm_cluster(const FieldParams& fp, const uint64_t* s, int64_t n, int R, uint64_t* b0, uint64_t* b1,
+                              int64_t* d_out, cudaStream_t st);
 size_t grid_sync_bytes();
 int grid_sync_err_offset();
 

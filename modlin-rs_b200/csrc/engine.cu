@@ -530,7 +530,21 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
     return MODLIN_OK;
   }
   int kernel = opts ? opts->kernel : MODLIN_LC_AUTO;
-  if (kernel == MODLIN_LC_AUTO) kernel = n >= 16384 ? MODLIN_LC_GRID : MODLIN_LC_BLOCK;
+  if (kernel == MODLIN_LC_AUTO)
+    kernel = n < 16384 ? MODLIN_LC_BLOCK : (bm_cluster_size((int64_t)n) ? MODLIN_LC_CLUSTER : MODLIN_LC_GRID);
+  if (kernel == MODLIN_LC_CLUSTER) {
+    const int R = bm_cluster_size((int64_t)n);
+    if (!R) return MODLIN_EINVAL_N;
+    CK(C->bmout.ensure(sizeof(int64_t) * 4));
+    CK(C->bmws.ensure((size_t)2 * n * 8));
+    uint64_t* b0 = C->bmws.as<uint64_t>();
+    CK(launch_bm_cluster(fp, d_s, (int64_t)n, R, b0, b0 + n, C->bmout.as<int64_t>(), st));
+    g_launches++;
+    CK(cudaMemcpyAsync(C->h_out, C->bmout.p, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *lc_out = (size_t)C->h_out[0];
+    return MODLIN_OK;
+  }
   CK(C->bmout.ensure(sizeof(int64_t) * 4));
   int64_t* d_out = C->bmout.as<int64_t>();
   if (kernel == MODLIN_LC_BLOCK) {

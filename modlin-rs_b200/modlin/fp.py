@@ -9,7 +9,7 @@ from ._lib import (Job, LcOpts, PROGRESS, RankOpts, check, lib, szt, u64p)
 from ._lib import Field as _CField
 
 KERNELS = {"auto": 0, "plain": 1, "tc": 2}
-LC_KERNELS = {"auto": 0, "block": 1, "grid": 2}
+LC_KERNELS = {"auto": 0, "block": 1, "grid": 2, "cluster": 3}
 _NO_PROGRESS = ctypes.cast(None, PROGRESS)
 
 

@@ -14,8 +14,15 @@ pytestmark = pytest.mark.gpu
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
 
 
+KINDS = ("block", "grid", "cluster")
+
+
 def lcs_all(M, p, s):
-    return {k: M.linear_complexity(p, s, kernel=k) for k in ("block", "grid")}
+    return {k: M.linear_complexity(p, s, kernel=k) for k in KINDS}
+
+
+def each(e):
+    return {k: e for k in KINDS}
 
 
 def test_linear_complexity_of_lfsr_sequence(M):
@@ -23,7 +30,7 @@ def test_linear_complexity_of_lfsr_sequence(M):
     s = [1, 2, 3]
     for i in range(3, 40):
         s.append((3 * s[i - 1] + 5 * s[i - 2] + 7 * s[i - 3]) % M61)
-    for k in ("block", "grid"):
+    for k in KINDS:
         assert M.linear_complexity(M61, s, kernel=k) == 3
         assert M.linear_complexity(M61, [4] * 20, kernel=k) == 1
         assert M.linear_complexity(M61, [0] * 20, kernel=k) == 0
@@ -37,19 +44,19 @@ def test_matches_reference(M, O):
         for n in [1, 2, 3, 5, 16, 50, 100, 200]:
             s = ts.lc_random(p, n)
             e = O.lc_naive(p, s)
-            assert lcs_all(M, p, s) == {"block": e, "grid": e}, (p, n)
+            assert lcs_all(M, p, s) == each(e), (p, n)
         for k in [1, 4, 10, 25]:
             s = ts.lc_lfsr(p, k)
             e = O.lc_naive(p, s)
             assert e <= k
-            assert lcs_all(M, p, s) == {"block": e, "grid": e}, (p, k)
+            assert lcs_all(M, p, s) == each(e), (p, k)
 
 
 def test_golden_lcs(M):
     for c in GOLD["oracle"]["lcs"]:
         p, n, L, seed = c["p"], c["n"], c["L"], c["seed"]
         s = M.gen.planted(p, L, seed, n) if L else M.gen.uniform(p, seed, n)
-        assert lcs_all(M, p, s) == {"block": c["lc"], "grid": c["lc"]}, c
+        assert lcs_all(M, p, s) == each(c["lc"]), c
 
 
 @pytest.mark.parametrize("p", [2, 127, 65521, 2147483647, M61, (1 << 62) + 135, (1 << 63) - 25])
@@ -57,7 +64,7 @@ def test_primes_vs_oracle(M, O, p):
     for n, L, seed in [(700, 0, 1), (1500, 90, 2), (4000, 1999, 3), (5000, 0, 4)]:
         s = O.gen_planted(p, L, seed, n) if L else O.gen_uniform(p, seed, n)
         e = O.linear_complexity(p, s)
-        assert lcs_all(M, p, s) == {"block": e, "grid": e}, (p, n, L)
+        assert lcs_all(M, p, s) == each(e), (p, n, L)
 
 
 def test_grid_kernel_cta_counts(M, O):
@@ -113,3 +120,23 @@ def test_input_validation(M):
     assert e.value.code == -3
     with pytest.raises(M.ModlinError):
         M.linear_complexity(0, [1])
+
+
+def test_cluster_kernel_long_sequences(M, O):
+    """The one-cluster kernel (16 CTAs, one cluster barrier per step) on long
+    sequences: equal to the oracle and to the grid kernel, for every field
+    policy, up to its length limit."""
+    for p, n, L, seed in [(M61, 40000, 0, 1), (65521, 30000, 7000, 2), ((1 << 63) - 25, 20000, 0, 3),
+                          (2147483647, 36000, 17000, 4)]:
+        s = O.gen_planted(p, L, seed, n) if L else O.gen_uniform(p, seed, n)
+        e = O.linear_complexity(p, s)
+        assert M.linear_complexity(p, s, kernel="cluster") == e, (p, n, L)
+        assert M.linear_complexity(p, s, kernel="grid") == e, (p, n, L)
+    import torch
+    n = 409600
+    t = torch.empty(n, dtype=torch.int64, device="cuda")
+    M.gen.planted_device(M61, 100000, 5, t.data_ptr(), n)
+    assert M.fp.linear_complexity_device(M61, t.data_ptr(), n, kernel="cluster") == 100000
+    with pytest.raises(M.ModlinError) as ex:
+        M.fp.linear_complexity_device(M61, t.data_ptr(), n + 1, kernel="cluster")
+    assert ex.value.code == -2
