@@ -85,7 +85,7 @@ __device__ int64_t bm_block_run(const F& f, const uint64_t* __restrict__ s, int6
       const uint64_t old = c[j];
       const int64_t jb = j - m;
       const uint64_t bj = (jb >= 0 && jb < bl) ? b[jb] : 0;
-      c[j] = f.reduce(f.prod(bb, old) + f.prod(nd, bj));
+      c[j] = f.reduce2(f.prod(bb, old) + f.prod(nd, bj));
       if (lenchg && j <= l) t[j] = old;
     }
     if (lenchg) {
@@ -267,7 +267,7 @@ __global__ void bm_grid_kernel(F f, const uint64_t* __restrict__ s, int64_t n, i
       const uint64_t old = cs[j - lo];
       const int64_t jb = j - m;
       const uint64_t bj = (jb >= 0 && jb < bl) ? __ldcg(bcur + jb) : 0;
-      cs[j - lo] = f.reduce(f.prod(bb, old) + f.prod(nd, bj));
+      cs[j - lo] = f.reduce2(f.prod(bb, old) + f.prod(nd, bj));
       if (lenchg && j <= l) __stcg(bnext + j, old);
     }
     if (lenchg) {
@@ -316,35 +316,37 @@ __global__ void __launch_bounds__(kClusterThreads, 1) bm_cluster_kernel(F f, con
   __shared__ uint64_t part[2][kClusterMax];  // [step parity][CTA]: partials pushed by every CTA
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int R = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-  const int64_t ntiles = (n + TH - 1) / TH;
-  const int my_tiles = ntiles > rank ? (int)((ntiles - rank + R - 1) / R) : 0;
+  // Indices fit in 32 bits here (n <= 409600).
+  const int nn = (int)n;
+  const int ntiles = (nn + TH - 1) / TH;
+  const int my_tiles = ntiles > rank ? (ntiles - rank + R - 1) / R : 0;
+  const int j0 = rank * TH + tid, jstride = R * TH;  // my index in tile k: j0 + k * jstride
   for (int k = 0; k < my_tiles; ++k) {
-    const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
-    cs[(k * TH) + tid] = j == 0;
-    if (j < n) bbuf0[j] = j == 0;
+    const int j = j0 + k * jstride;
+    cs[k * TH + tid] = j == 0;
+    if (j < nn) bbuf0[j] = j == 0;
   }
   uint64_t* part_dst = lane < R ? cl.map_shared_rank(&part[0][rank], lane) : nullptr;
   cl.sync();
-  const uint64_t sb = f.safe_batch();
   uint64_t* bcur = bbuf0;
   uint64_t* bnext = bbuf1;
-  int64_t l = 0, m = 1, bl = 1;
+  int l = 0, m = 1, bl = 1;
   uint64_t bb = 1;
-  for (int64_t i = 0; i < n; ++i) {
+  for (int i = 0; i < nn; ++i) {
     // Partial discrepancy over my indices j <= l; the loads of a batch of
     // tiles are issued together so that one L2 latency covers them.
     uint64_t tot = 0;
-    const int kend = (int)(l < 0 ? 0 : ((l / TH) - rank + R) / R);  // tiles that may hold j <= l
+    const int kend = (l / TH - rank + R) / R;  // tiles that may hold j <= l
     const int kn = kend < my_tiles ? kend : my_tiles;
     for (int k0 = 0; k0 < kn; k0 += kTileBatch) {
       uint64_t sv[kTileBatch], cv[kTileBatch];
 #pragma unroll
       for (int q = 0; q < kTileBatch; ++q) {
         const int k = k0 + q;
-        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+        const int j = j0 + k * jstride;
         const bool on = k < kn && j <= l;
         sv[q] = on ? s[i - j] : 0;
-        cv[q] = on ? cs[(k * TH) + tid] : 0;
+        cv[q] = on ? cs[k * TH + tid] : 0;
       }
       // Two independent chains of kTileBatch / 2 <= 4 <= safe_batch
       // products each (p < 2^63), reduced at the end of the batch.
@@ -378,27 +380,27 @@ __global__ void __launch_bounds__(kClusterThreads, 1) bm_cluster_kernel(F f, con
     }
     const bool lenchg = 2 * l <= i;
     const uint64_t nd = f.modulus() - d;  // c <- bb c + (p - d) x^m b: one reduction per entry
-    int64_t uhi = l + 1 > m + bl ? l + 1 : m + bl;
-    if (uhi > n) uhi = n;
-    const int kuend = (int)(((uhi - 1) / TH) - rank + R) / R;  // tiles that may hold j < uhi
+    int uhi = l + 1 > m + bl ? l + 1 : m + bl;
+    if (uhi > nn) uhi = nn;
+    const int kuend = ((uhi - 1) / TH - rank + R) / R;  // tiles that may hold j < uhi
     const int ku = kuend < my_tiles ? kuend : my_tiles;
     for (int k0 = 0; k0 < ku; k0 += kTileBatch) {
       uint64_t bv[kTileBatch];
 #pragma unroll
       for (int q = 0; q < kTileBatch; ++q) {
         const int k = k0 + q;
-        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
-        const int64_t jb = j - m;
+        const int j = j0 + k * jstride;
+        const int jb = j - m;
         bv[q] = (k < ku && j < uhi && jb >= 0 && jb < bl) ? __ldcg(bcur + jb) : 0;
       }
 #pragma unroll
       for (int q = 0; q < kTileBatch; ++q) {
         const int k = k0 + q;
-        const int64_t j = (((int64_t)k * R + rank) * TH) + tid;
+        const int j = j0 + k * jstride;
         if (k < ku && j < uhi) {
-          uint64_t* cp = cs + (k * TH) + tid;
+          uint64_t* cp = cs + k * TH + tid;
           const uint64_t old = *cp;
-          *cp = f.reduce(f.prod(bb, old) + f.prod(nd, bv[q]));
+          *cp = f.reduce2(f.prod(bb, old) + f.prod(nd, bv[q]));
           if (lenchg && j <= l) __stcg(bnext + j, old);
         }
       }

@@ -75,6 +75,8 @@ struct FpBarrett {
   MODLIN_HD uint64_t mul(uint64_t a, uint64_t b) const { return reduce((u128)a * b); }
   // Full product of two residues, for lazy accumulation.
   MODLIN_HD u128 prod(uint64_t a, uint64_t b) const { return (u128)a * b; }
+  // Exact residue of a sum of at most two products of residues.
+  MODLIN_HD uint64_t reduce2(u128 t) const { return reduce(t); }
   // Number of (p-1)^2 products a u128 accumulator holds before it must be reduced.
   MODLIN_HD uint64_t safe_batch() const { return sb; }
   MODLIN_HD uint64_t modulus() const { return p; }
@@ -88,6 +90,7 @@ struct FpSmall {
   FpSmall() = default;
   MODLIN_HD explicit FpSmall(const FieldParams& f) : wide(f) {}
   MODLIN_HD uint64_t reduce(u128 t) const { return wide.reduce(t); }
+  MODLIN_HD uint64_t reduce2(u128 t) const { return wide.reduce(t); }
   MODLIN_HD uint64_t reduce64(uint64_t x) const {
     const uint64_t q = (uint64_t)(((u128)x * wide.mu_hi) >> 64);
     uint64_t r = x - q * wide.p;
@@ -133,6 +136,15 @@ struct FpM61 {
     return x >= kM61 ? x - kM61 : x;
   }
   MODLIN_HD u128 prod(uint64_t a, uint64_t b) const { return (u128)a * b; }
+  // t < 2^123 (a sum of at most two products of residues): t = hi 2^64 + lo
+  // with hi < 2^59, and 2^64 = 8 (mod p), so (lo mod 2^61) + (lo >> 61) +
+  // 8 hi < 2^63 needs one more fold.
+  MODLIN_HD uint64_t reduce2(u128 t) const {
+    const uint64_t lo = (uint64_t)t, hi = (uint64_t)(t >> 64);
+    uint64_t x = (lo & kM61) + (lo >> 61) + (hi << 3);
+    x = fold(x);
+    return x >= kM61 ? x - kM61 : x;
+  }
   MODLIN_HD uint64_t safe_batch() const { return 64; }
   MODLIN_HD uint64_t modulus() const { return kM61; }
 };

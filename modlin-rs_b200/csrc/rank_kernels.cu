@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int k = s + 16 * q;
-        M[j][k] = k == c ? f.mul(nh, spiv) : f.reduce(f.prod(e, M[j][k]) + f.prod(nh, M[piv][k]));
+        M[j][k] = k == c ? f.mul(nh, spiv) : f.reduce2(f.prod(e, M[j][k]) + f.prod(nh, M[piv][k]));
       }
       if (s == 0) {
         if ((used >> j) & 1)
