@@ -19,7 +19,7 @@ import os
 
 from . import _lib
 from ._lib import ModlinError, lib, library_path  # noqa: F401
-from . import fp, prng, stats, gen  # noqa: F401
+from . import fp, prng, stats, gen, shard  # noqa: F401
 from .fp import Field, rank, linear_complexity, rank_batch, lc_batch  # noqa: F401
 from .stats import corank_prob, corank_tail_pvalue, lc_left_tail_pvalue, pretty_p_value  # noqa: F401
 
