@@ -676,8 +676,18 @@ def main():
                 peak = 2 * peaks.get("bf16_tflops", 1590.0)
                 peak_note = "2 x measured bf16 dense (MEASURED_PEAKS.json); int8 GEMM unavailable"
             achieved = Wtr * 64 * 2 / (tr_ms * 1e-3) / 1e12
+            # DRAM traffic per launch: ncu (dram__bytes_read + dram__bytes_write) of
+            # the first wide K = 128 update of the 8192^2 rank was 550.0 + 454.4 MB
+            # for 8064 x 7936 outputs (15.69 B per output against 16 algorithmic:
+            # C read + write); scaled to this run's average launch by its outputs.
+            outputs_per_launch = Wtr / depth / max(n_tr, 1)
+            traffic = 15.69 * outputs_per_launch
             roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None, "kernel": "trailing_tc (tcgen05 kind::i8)",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "traffic_note": "bytes per launch: ncu DRAM bytes per output of an 8192^2 wide update "
+                                    "x outputs per launch here (algorithmic: 16 B per output)",
+                    "hbm_gbs_of_c": 16 * outputs_per_launch / (per_launch_ms * 1e-3) / 1e9,
+                    "kernel": "trailing_tc (tcgen05 kind::i8)",
                     "peak_source": peak_note,
                     "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops "
                                               f"(K = {depth}, {n_tr} updates per rank)",
