@@ -64,3 +64,13 @@ def test_reps_match_one_at_a_time(O):
         c = 40 - O.rank(97, x[1600 * t:1600 * (t + 1)], 40)
         p = O.pretty_p_value(O.corank_tail_pvalue(97, 40, c))
         assert out[3 + t] == f"Matrix {t + 1}/3\tcorank={c}\tp={p}"
+
+
+def test_readme_headline_mixmax256_rank_65536():
+    """README.md:110-113: MIXMAX-256 fails the rank test once the side
+    exceeds its linear complexity 65280 (README.md:98-107). The largest run
+    here: a 65536 x 65536 matrix (32 GiB) over 2^61-1 from MIXMAX-256 seed 1
+    has corank 65536 - 65280 = 256."""
+    out = run("-R", "65536", "-p", str(M61), "-S", "1", "--prng", "mixmax256")
+    assert out[0] == "Generator: MIXMAX (TRandomMixMax256, N=256, skip=2)"
+    assert out[-1] == "Matrix 1/1\tcorank=256\tp=1e-307"
