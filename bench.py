@@ -516,6 +516,7 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default AUTO choices")
     ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch", "rank-planted"],
                     help="rank: the 16384^2 rank (default line); bm / rank-batch: only those measurements")
     args = ap.parse_args()
@@ -536,6 +537,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     import modlin
     from modlin import fp as mfp
+
+    # The AUTO choices measured on this GPU (a few seconds, before any timing).
+    tune = modlin.autotune()["choice"] if not args.no_autotune else None
 
     if args.workload == "bm":
         res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
@@ -719,7 +723,8 @@ def main():
             "config": {"workload": f"single large rank {n}x{n} over p=2^61-1, uniform SplitMix64({7}+rank) "
                                    "residues, resident in HBM", "n": n, "p": M61, "kernel": kernel,
                        "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs (2 GiB) larger than L2", "rank": r, "work_modmac": W},
+                       "l2": "inputs (2 GiB) larger than L2", "rank": r, "work_modmac": W,
+                       "autotuned": tune},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(), **extras,
         }

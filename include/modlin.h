@@ -213,6 +213,20 @@ int modlin_gen_planted_batch_device(const uint64_t *p, const size_t *L, const ui
 /* Field::reduce on the device, in place (src/main.rs:94-104 fill). */
 int modlin_reduce_device(uint64_t p, uint64_t *d_x, size_t count, void *stream);
 
+/* ---- Autotuning ----------------------------------------------------------- */
+
+/* Measures, on the current device, the choices MODLIN_RANK_AUTO and
+ * MODLIN_LC_AUTO make (no reference counterpart: the reference has one CPU
+ * path): the side from which the tensor-core trailing update beats the plain
+ * one, per limb count (1, 2, 4 or 8 limbs for p below 2^8, 2^16, 2^32, 2^63;
+ * the limb count itself is the smallest exact one); the smallest side for
+ * two-panel block steps; Berlekamp-Massey threads per CTA by length, the
+ * block/cluster crossover, and batch threads per CTA by the longest sequence.
+ * Takes a few seconds; the choices hold for this process and device. `report`
+ * (may be NULL) receives them and the timings as JSON, truncated to cap - 1
+ * characters. Before any call, fixed defaults apply. */
+int modlin_autotune(char *report, size_t cap);
+
 /* ---- Diagnostics --------------------------------------------------------- */
 
 /* Number of this library's kernel launches since load (for launch-count

@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) bm_cluster_kernel(F f, con
 cudaError_t launch_bm_block(const BmJob& job, uint64_t* gws, int64_t smem_words, int threads, int64_t* d_out,
                             cudaStream_t st) {
   const size_t smem = (3 * job.n <= smem_words) ? (size_t)(3 * job.n) * 8 : 0;
-  if (smem > 48 * 1024)
+  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
     cudaFuncSetAttribute(bm_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   bm_block_kernel<<<1, threads, smem, st>>>(job, gws, smem_words, d_out);
   return cudaGetLastError();
@@ -437,7 +437,7 @@ cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long lo
                             int64_t gws_words, int64_t smem_words, int blocks, int threads, int64_t* d_out,
                             cudaStream_t st) {
   const size_t smem = (size_t)smem_words * 8;
-  if (smem > 48 * 1024)
+  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
     cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   bm_batch_kernel<<<blocks, threads, smem, st>>>(d_jobs, count, d_next, gws, gws_words, smem_words, d_out);
   return cudaGetLastError();
@@ -445,7 +445,7 @@ cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long lo
 
 int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words) {
   const size_t smem = (size_t)smem_words * 8;
-  if (smem > 48 * 1024)
+  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
     cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nb = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bm_batch_kernel, threads, smem);
@@ -458,7 +458,7 @@ static cudaError_t launch_grid_t(const F& f, const uint64_t* s, int64_t n, int c
                                  int* ctas_used) {
   const int64_t chunk = (n + ctas - 1) / ctas;
   const size_t smem = (size_t)chunk * 8;
-  if (smem > 48 * 1024)
+  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
     cudaFuncSetAttribute(bm_grid_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm_grid_kernel<F>, threads, smem);

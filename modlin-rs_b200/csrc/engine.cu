@@ -10,6 +10,7 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "../../include/modlin.h"
@@ -47,8 +48,29 @@ struct DevBuf {
   }
 };
 
+// Choices the autotuner measures (defaults until modlin_autotune runs on the
+// device): plain/tensor-core crossover per limb count, smallest side for
+// two-panel block steps, BM threads per CTA by length, BM block/cluster
+// crossover, BM batch threads by the longest sequence.
+struct Tune {
+  bool measured = false;
+  int tc_cross[4] = {512, 512, 512, 512};           // 1, 2, 4, 8 limbs
+  int two_panel_min = 256;
+  int bm_threads[4] = {256, 256, 1024, 1024};       // n < 1024, < 4096, < 16384, longer
+  int bm_cluster_min = 16384;
+  int bm_batch_threads[3] = {128, 256, 512};        // longest < 512, < 2048, longer
+};
+
+static int limb_class(uint64_t p) {
+  const int bits = 64 - __builtin_clzll(p - 1);
+  return bits <= 8 ? 0 : bits <= 16 ? 1 : bits <= 32 ? 2 : 3;
+}
+static int bm_len_class(size_t n) { return n < 1024 ? 0 : n < 4096 ? 1 : n < 16384 ? 2 : 3; }
+static int bm_batch_class(int64_t maxn) { return maxn < 512 ? 0 : maxn < 2048 ? 1 : 2; }
+
 struct Ctx {
   int device = -1;
+  Tune tune;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
   std::mutex mu;
@@ -67,6 +89,7 @@ struct Ctx {
   DevBuf gena, genjobs;  // planted-generator coefficients and jobs
   DevBuf jump;           // jump-ahead scratch of the long planted generator
   DevBuf batchm, rbjobs, rbout;  // batched rank: matrix arena, jobs, ranks
+  DevBuf tunebuf;                // autotuner inputs
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
 };
@@ -137,12 +160,13 @@ struct RankRun {
   std::vector<int>* pcols;
   modlin_progress_fn cb;
   void* cb_ctx;
+  int two_panel_min;  // smallest side for two-panel steps (tensor-core path)
 };
 
 static bool use_tc(const RankRun& R) {
   if (R.kernel == MODLIN_RANK_PLAIN) return false;
   if (R.kernel == MODLIN_RANK_TC) return true;
-  return R.n >= tc_crossover_n(R.fp->p);
+  return R.n >= R.ctx->tune.tc_cross[limb_class(R.fp->p)];
 }
 
 template <class F>
@@ -248,7 +272,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     const int jend = std::min(col + kPanel, n);
     const int W = jend - col;
     const int r0 = rank;
-    if (tc && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
+    if (tc && n >= R.two_panel_min && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
       // Two-panel block step: P = A[r0 .. r0+128, col .. col+128) split into
       // 64 x 64 blocks [P11 P12; P21 P22]. With V11 = P11^-1 and the Schur
       // complement S = P22 - P21 V11 P12 invertible, the multipliers of the
@@ -501,7 +525,7 @@ static int rank_device_locked(Ctx* C, uint64_t p, uint64_t* d_m, size_t n, const
   if (!rank_out) return MODLIN_EINVAL_ARG;
   std::vector<int> pc;
   RankRun R{&fp, d_m, (int)n, opts ? opts->kernel : MODLIN_RANK_AUTO, st, C, pivot_cols_out ? &pc : nullptr,
-            cb, cb_ctx};
+            cb, cb_ctx, C->tune.two_panel_min};
   const int rc = p == kM61 ? rank_impl<FpM61>(R, rank_out) : rank_impl<FpBarrett>(R, rank_out);
   if (rc != MODLIN_OK) return rc;
   if (pivot_cols_out) {
@@ -531,7 +555,8 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
   }
   int kernel = opts ? opts->kernel : MODLIN_LC_AUTO;
   if (kernel == MODLIN_LC_AUTO)
-    kernel = n < 16384 ? MODLIN_LC_BLOCK : (bm_cluster_size((int64_t)n) ? MODLIN_LC_CLUSTER : MODLIN_LC_GRID);
+    kernel = (int64_t)n < C->tune.bm_cluster_min ? MODLIN_LC_BLOCK
+             : (bm_cluster_size((int64_t)n) ? MODLIN_LC_CLUSTER : MODLIN_LC_GRID);
   if (kernel == MODLIN_LC_CLUSTER) {
     const int R = bm_cluster_size((int64_t)n);
     if (!R) return MODLIN_EINVAL_N;
@@ -551,7 +576,7 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
     const int64_t smem_words = (200 * 1024) / 8;
     if (3 * (int64_t)n > smem_words) CK(C->bmws.ensure((size_t)3 * n * 8));
     BmJob job{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_s, (int64_t)n, 0};
-    CK(launch_bm_block(job, C->bmws.as<uint64_t>(), smem_words, n >= 4096 ? 1024 : 256, d_out, st));
+    CK(launch_bm_block(job, C->bmws.as<uint64_t>(), smem_words, C->tune.bm_threads[bm_len_class(n)], d_out, st));
     g_launches++;
   } else {
     int ctas = opts && opts->grid_ctas > 0 ? opts->grid_ctas : C->num_sms;
@@ -645,7 +670,7 @@ static int lc_batch_locked(Ctx* C, const uint64_t* p, const uint64_t* const* d_d
   }
   // Longest first: the persistent CTAs then finish close together (LPT).
   std::stable_sort(jobs.begin(), jobs.end(), [](const BmJob& a, const BmJob& b) { return a.n > b.n; });
-  const int threads = maxn > 2048 ? 512 : (maxn > 512 ? 256 : 128);
+  const int threads = C->tune.bm_batch_threads[bm_batch_class(maxn)];
   int64_t smem_words = std::min<int64_t>(3 * maxn, (200 * 1024) / 8);
   int per_sm = bm_batch_max_blocks_per_sm(threads, smem_words);
   if (per_sm < 1) per_sm = 1;
@@ -665,6 +690,242 @@ static int lc_batch_locked(Ctx* C, const uint64_t* p, const uint64_t* const* d_d
   CK(cudaMemcpyAsync(out.data(), C->bmout.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   for (size_t i = 0; i < count; ++i) lcs_out[i] = (size_t)out[i];
+  return MODLIN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: measures the AUTO choices on this device (CUDA events on the
+// library stream, best of a few runs) and stores them in the context.
+// ---------------------------------------------------------------------------
+template <class Fn>
+static float best_ms(Ctx* C, int reps, Fn&& fn, int* rc_out) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float best = 1e30f;
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(a, C->stream);
+    const int rc = fn();
+    cudaEventRecord(b, C->stream);
+    cudaEventSynchronize(b);
+    if (rc != MODLIN_OK) {
+      *rc_out = rc;
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+// Smallest candidate from which `faster` holds for it and every larger one
+// (sizes ascending); `none` when it never does.
+static int crossover(const std::vector<int>& sizes, const std::vector<bool>& faster, int none) {
+  int cross = none;
+  for (int i = (int)sizes.size() - 1; i >= 0 && faster[i]; --i) cross = sizes[i];
+  return cross;
+}
+
+// A failed step leaves its name and the CUDA error in the report.
+#define TK(expr)                                                                        \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess) {                                                            \
+      rep += std::string("\"error\": \"") + #expr + ": " + cudaGetErrorName(_e) + "\"}"; \
+      return cuda_rc(_e);                                                               \
+    }                                                                                   \
+  } while (0)
+
+static int autotune_locked(Ctx* C, std::string& rep) {
+  int rc = MODLIN_OK;
+  cudaStream_t st = C->stream;
+  Tune T = C->tune;
+  char buf[256];
+  rep = "{";
+  // 1. Plain vs tensor-core rank per limb count (uniform matrices).
+  const uint64_t primes[4] = {127, 65521, 2147483647ULL, kM61};
+  const std::vector<int> sizes = {64, 96, 128, 192, 256, 384, 512, 768, 1024};
+  const int nmax = 16384;  // largest side measured (two-panel steps)
+  TK(C->tunebuf.ensure((size_t)nmax * nmax * 8));
+  TK(C->mat.ensure((size_t)nmax * nmax * 8));
+  uint64_t* pristine = C->tunebuf.as<uint64_t>();
+  uint64_t* work = C->mat.as<uint64_t>();
+  rep += "\"rank_ms\": {";
+  for (int li = 0; li < 4; ++li) {
+    const uint64_t p = primes[li];
+    std::vector<bool> tc_wins;
+    for (int n : sizes) {
+      uint64_t nl = 0;
+      TK(gen_uniform_device(p, 1234 + n, pristine, (uint64_t)n * n, st, &nl));
+      float t[2];
+      for (int k = 0; k < 2; ++k) {
+        const modlin_rank_opts o{k == 0 ? MODLIN_RANK_PLAIN : MODLIN_RANK_TC, 0};
+        size_t r = 0;
+        t[k] = best_ms(C, 2, [&]() -> int {
+          if (cudaMemcpyAsync(work, pristine, (size_t)n * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return MODLIN_ECUDA;
+          return rank_device_locked(C, p, work, n, &o, &r, nullptr, st, nullptr, nullptr);
+        }, &rc);
+        if (rc) return rc;
+      }
+      tc_wins.push_back(t[1] <= t[0]);
+      std::snprintf(buf, sizeof buf, "%s\"%d-limb n=%d\": [%.3f, %.3f]", rep.back() == '{' ? "" : ", ",
+                    1 << li, n, t[0], t[1]);
+      rep += buf;
+    }
+    T.tc_cross[li] = crossover(sizes, tc_wins, 1 << 30);
+  }
+  rep += "}";
+  // 2. Two-panel steps against one-panel steps (tensor cores, 2^61 - 1).
+  {
+    const std::vector<int> tsz = {256, 512, 1024, 2048, 4096, 8192, 12288, 16384};
+    std::vector<bool> two_wins;
+    rep += ", \"two_panel_ms\": {";
+    const int saved = C->tune.two_panel_min;
+    for (int n : tsz) {
+      uint64_t nl = 0;
+      TK(gen_uniform_device(kM61, 99 + n, pristine, (uint64_t)n * n, st, &nl));
+      float t[2];
+      for (int k = 0; k < 2; ++k) {
+        C->tune.two_panel_min = k == 0 ? (1 << 30) : 0;
+        const modlin_rank_opts o{MODLIN_RANK_TC, 0};
+        size_t r = 0;
+        t[k] = best_ms(C, 2, [&]() -> int {
+          if (cudaMemcpyAsync(work, pristine, (size_t)n * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return MODLIN_ECUDA;
+          return rank_device_locked(C, kM61, work, n, &o, &r, nullptr, st, nullptr, nullptr);
+        }, &rc);
+      }
+      C->tune.two_panel_min = saved;
+      if (rc) return rc;
+      two_wins.push_back(t[1] <= t[0]);
+      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == tsz[0] ? "" : ", ", n, t[0], t[1]);
+      rep += buf;
+    }
+    rep += "}";
+    T.two_panel_min = crossover(tsz, two_wins, 1 << 30);
+  }
+  // 3. BM: threads per CTA of the block kernel by length class, then the
+  //    block/cluster crossover.
+  FieldParams fp;
+  make_field_params(kM61, &fp);
+  const int64_t bm_len[4] = {768, 3072, 12288, 32768};
+  const int thr[4] = {128, 256, 512, 1024};
+  TK(C->seq.ensure((size_t)65536 * 8));
+  TK(C->bmout.ensure(sizeof(int64_t) * 4));
+  TK(C->bmws.ensure((size_t)3 * 65536 * 8));
+  uint64_t* seq = C->seq.as<uint64_t>();
+  const int64_t smem_words = (200 * 1024) / 8;
+  rep += ", \"bm_block_ms\": {";
+  for (int c = 0; c < 4; ++c) {
+    uint64_t nl = 0;
+    TK(gen_uniform_device(kM61, 555 + c, seq, (uint64_t)bm_len[c], st, &nl));
+    float best = 1e30f;
+    for (int t : thr) {
+      BmJob job{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, seq, bm_len[c], 0};
+      const float ms = best_ms(C, 2, [&]() -> int {
+        const cudaError_t e = launch_bm_block(job, C->bmws.as<uint64_t>(), smem_words, t, C->bmout.as<int64_t>(), st);
+        if (e != cudaSuccess) rep += std::string("\"error\": \"bm block t=") + std::to_string(t) + ": " +
+                                     cudaGetErrorName(e) + "\", ";
+        return e == cudaSuccess ? MODLIN_OK : MODLIN_ECUDA;
+      }, &rc);
+      if (rc) return rc;
+      std::snprintf(buf, sizeof buf, "%s\"n=%lld t=%d\": %.3f", rep.back() == '{' ? "" : ", ",
+                    (long long)bm_len[c], t, ms);
+      rep += buf;
+      if (ms < best) {
+        best = ms;
+        T.bm_threads[c] = t;
+      }
+    }
+  }
+  rep += "}, \"bm_cluster_ms\": {";
+  {
+    const std::vector<int> csz = {4096, 8192, 16384, 32768, 65536};
+    std::vector<bool> cl_wins;
+    for (int n : csz) {
+      uint64_t nl = 0;
+      TK(gen_uniform_device(kM61, 777 + n, seq, (uint64_t)n, st, &nl));
+      BmJob job{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, seq, n, 0};
+      const int tb = T.bm_threads[bm_len_class(n)];
+      const float tblk = best_ms(C, 1, [&]() -> int {
+        return launch_bm_block(job, C->bmws.as<uint64_t>(), smem_words, tb, C->bmout.as<int64_t>(), st) ==
+                       cudaSuccess
+                   ? MODLIN_OK
+                   : MODLIN_ECUDA;
+      }, &rc);
+      if (rc) return rc;
+      const float tcl = best_ms(C, 1, [&]() -> int {
+        uint64_t* b0 = C->bmws.as<uint64_t>();
+        const cudaError_t e = launch_bm_cluster(fp, seq, n, bm_cluster_size(n), b0, b0 + n, C->bmout.as<int64_t>(), st);
+        if (e != cudaSuccess) rep += std::string("\"error\": \"bm cluster n=") + std::to_string(n) + ": " +
+                                     cudaGetErrorName(e) + "\", ";
+        return e == cudaSuccess ? MODLIN_OK : MODLIN_ECUDA;
+      }, &rc);
+      if (rc) return rc;
+      cl_wins.push_back(tcl <= tblk);
+      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == csz[0] ? "" : ", ", n, tblk, tcl);
+      rep += buf;
+    }
+    T.bm_cluster_min = crossover(csz, cl_wins, 1 << 30);
+  }
+  rep += "}";
+  // 4. BM batches: threads per CTA by the longest sequence.
+  {
+    const int64_t lo[3] = {64, 512, 2048}, hi[3] = {512, 2048, 8192};
+    const int bthr[3] = {128, 256, 512};
+    const int count = C->num_sms * 6;
+    std::vector<size_t> ns(count);
+    std::vector<const uint64_t*> ptrs(count);
+    std::vector<uint64_t> ps(count, kM61);
+    std::vector<size_t> out(count);
+    TK(C->tunebuf.ensure((size_t)count * 8192 * 8));
+    uint64_t* arena = C->tunebuf.as<uint64_t>();
+    uint64_t nl = 0;
+    TK(gen_uniform_device(kM61, 4242, arena, (uint64_t)count * 8192, st, &nl));
+    rep += ", \"bm_batch_ms\": {";
+    for (int c = 0; c < 3; ++c) {
+      uint64_t z = 0x1234 + c;
+      for (int i = 0; i < count; ++i) {
+        z = z * 6364136223846793005ULL + 1442695040888963407ULL;
+        ns[i] = (size_t)(lo[c] + (int64_t)((z >> 33) % (uint64_t)(hi[c] - lo[c])));
+        ptrs[i] = arena + (size_t)i * 8192;
+      }
+      float best = 1e30f;
+      const int saved = C->tune.bm_batch_threads[c];
+      for (int t : bthr) {
+        C->tune.bm_batch_threads[c] = t;
+        const float ms = best_ms(C, 1, [&]() -> int {
+          return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, out.data(), st);
+        }, &rc);
+        if (rc) {
+          C->tune.bm_batch_threads[c] = saved;
+          return rc;
+        }
+        std::snprintf(buf, sizeof buf, "%s\"max<%lld t=%d\": %.3f", rep.back() == '{' ? "" : ", ",
+                      (long long)hi[c], t, ms);
+        rep += buf;
+        if (ms < best) {
+          best = ms;
+          T.bm_batch_threads[c] = t;
+        }
+      }
+      C->tune.bm_batch_threads[c] = saved;
+    }
+    rep += "}";
+  }
+  T.measured = true;
+  C->tune = T;
+  std::snprintf(buf, sizeof buf,
+                ", \"choice\": {\"tc_crossover\": [%d, %d, %d, %d], \"two_panel_min\": %d, "
+                "\"bm_threads\": [%d, %d, %d, %d], \"bm_cluster_min\": %d, \"bm_batch_threads\": [%d, %d, %d]}}",
+                T.tc_cross[0], T.tc_cross[1], T.tc_cross[2], T.tc_cross[3], T.two_panel_min, T.bm_threads[0],
+                T.bm_threads[1], T.bm_threads[2], T.bm_threads[3], T.bm_cluster_min, T.bm_batch_threads[0],
+                T.bm_batch_threads[1], T.bm_batch_threads[2]);
+  rep += buf;
   return MODLIN_OK;
 }
 
@@ -1122,5 +1383,20 @@ uint64_t modlin_kernel_launches(void) { return g_launches.load(); }
 double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
 
 double modlin_last_trailing_macs(void) { return g_last_trailing_macs; }
+
+int modlin_autotune(char* report, size_t cap) {
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  std::string rep;
+  rc = autotune_locked(C, rep);
+  if (report && cap) {
+    const size_t k = std::min(cap - 1, rep.size());
+    std::memcpy(report, rep.data(), k);
+    report[k] = 0;
+  }
+  return rc;
+}
 
 }  // extern "C"

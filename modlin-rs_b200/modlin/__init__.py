@@ -37,3 +37,14 @@ def last_trailing_ms() -> float:
 def last_trailing_macs() -> float:
     """Modular multiply-adds done by those timed trailing updates."""
     return float(lib().modlin_last_trailing_macs())
+
+
+def autotune() -> dict:
+    """Measure this device's AUTO choices (a few seconds); returns the choices
+    and the timings they came from."""
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    rc = lib().modlin_autotune(buf, len(buf))
+    if rc != 0:
+        raise ModlinError(rc, "autotune: " + buf.value.decode(errors="replace")[-400:])
+    return json.loads(buf.value.decode())

@@ -96,6 +96,7 @@ def lib():
     _proto(L, "modlin_kernel_launches", u64, [])
     _proto(L, "modlin_last_trailing_ms", ctypes.c_double, [])
     _proto(L, "modlin_last_trailing_macs", ctypes.c_double, [])
+    _proto(L, "modlin_autotune", ci, [ctypes.c_char_p, szt])
     _lib = L
     return L
 
@@ -116,5 +117,5 @@ EXPORTED = [
     "modlin_prng_new", "modlin_prng_name", "modlin_prng_fill", "modlin_prng_free",
     "modlin_gen_uniform", "modlin_gen_uniform_device", "modlin_gen_planted", "modlin_reduce_device",
     "modlin_gen_planted_device", "modlin_gen_planted_batch_device",
-    "modlin_kernel_launches", "modlin_last_trailing_ms", "modlin_last_trailing_macs",
+    "modlin_kernel_launches", "modlin_last_trailing_ms", "modlin_last_trailing_macs", "modlin_autotune",
 ]

@@ -140,3 +140,14 @@ def test_cluster_kernel_long_sequences(M, O):
     with pytest.raises(M.ModlinError) as ex:
         M.fp.linear_complexity_device(M61, t.data_ptr(), n + 1, kernel="cluster")
     assert ex.value.code == -2
+
+
+def test_shared_memory_boundary_lengths(M, O):
+    """Lengths whose c, b, t arrays need just under 48 KiB of dynamic shared
+    memory: with the kernels' static shared memory the total passes 48 KiB
+    (the launch must opt in)."""
+    for n in [2027, 2040, 2047, 2048]:
+        s = O.gen_uniform(65521, n, n)
+        e = O.linear_complexity(65521, s)
+        assert M.linear_complexity(65521, s, kernel="block") == e, n
+        assert M.lc_batch([(65521, s), (M61, O.gen_uniform(M61, 1, 100))])[0] == e, n
