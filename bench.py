@@ -235,11 +235,12 @@ def bm_batch_build(torch, modlin, jobs, iid_seeds):
 
 
 def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, batch_count=65536,
-               plain_sample=512):
+               plain_sample=512, cpu=True):
     """Berlekamp-Massey throughput (steps = sequence elements processed):
-    the two long sequences on the cooperative grid kernel, the batch in one
-    persistent launch, and the plain one-sequence-per-launch form on a
-    sample of the same batch."""
+    the two long sequences on the cluster and grid kernels, the batch in one
+    persistent launch, the plain one-sequence-per-launch form on a sample of
+    the same batch and, with `cpu`, the oracle (the reference's single-
+    threaded algorithm) on bounded samples of both."""
     from modlin import fp as mfp
     res = {}
     for name, planted, seed in (("long_planted", True, 21), ("long_iid", False, 22)):
@@ -301,6 +302,28 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     batch["plain_one_per_launch"] = {"sequences": len(idx), "steps": sub, "ms": pms,
                                      "steps_per_s": sub / (pms * 1e-3)}
     batch["speedup_vs_plain"] = batch["steps_per_s"] / batch["plain_one_per_launch"]["steps_per_s"]
+    if cpu:
+        # The reference runs BM single-threaded, one sequence after another.
+        import oracle
+        oracle.build()
+        sample = idx[:48]
+        base = ptrs[0]
+        host = arena.cpu().numpy().view("uint64")
+        t0 = time.perf_counter()
+        for i in sample:
+            o = (ptrs[i] - base) // 8
+            assert oracle.linear_complexity(ps[i], host[o:o + ns[i]]) == lcs[i]
+        dt = time.perf_counter() - t0
+        steps_cpu = sum(ns[i] for i in sample)
+        batch["cpu_oracle_one_thread"] = {"sequences": len(sample), "steps": steps_cpu, "s": dt,
+                                          "steps_per_s": steps_cpu / dt}
+        nl = 40000
+        t = modlin.gen.uniform(M61, 22, nl)
+        t0 = time.perf_counter()
+        oracle.linear_complexity(M61, t)
+        dt = time.perf_counter() - t0
+        res["long_iid"]["cpu_oracle_one_thread"] = {"n": nl, "s": dt, "steps_per_s": nl / dt,
+                                                    "note": "prefix of length 40000 of the same stream"}
     res["batch"] = batch
     del arena
     return res
@@ -629,7 +652,8 @@ def main():
             extras["plain_modmac_per_s"] = W / (e0.elapsed_time(e1) * 1e-3)
             extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
         # Berlekamp-Massey: the long sequences and the 65536-sequence batch.
-        extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128)
+        extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128,
+                                                cpu=not args.no_cpu_baseline)
         # The planted large rank (order-4096 recurrence windows, rank 4096).
         extras["rank_planted"] = rank_planted_measure(torch, modlin)
         # Batched rank: 4096 matrices of sides 64..1024 in one launch.
