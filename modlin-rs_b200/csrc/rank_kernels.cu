@@ -391,8 +391,9 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int k = s + 16 * q;
-        M[j][k] = k == c ? f.mul(nh, spiv) : f.reduce2(f.prod(e, M[j][k]) + f.prod(nh, M[piv][k]));
+        M[j][k] = f.reduce2(f.prod(e, M[j][k]) + f.prod(nh, M[piv][k]));
       }
+      if (s == (c & 15)) M[j][c] = f.mul(nh, spiv);  // column c now holds E's column piv
       if (s == 0) {
         if ((used >> j) & 1)
           d[j] = f.mul(e, d[j]);
@@ -445,19 +446,23 @@ __global__ void __launch_bounds__(kInvThreads) small_gemm64_kernel(F f, const ui
   }
   __syncthreads();
   const uint64_t p = f.modulus(), sb = f.safe_batch();
+  // Four independent accumulators (one per output column of this thread).
+  u128 acc[4] = {0, 0, 0, 0};
+  uint64_t cnt = 0;
+  for (int k = 0; k < kPanel; ++k) {
+    const uint64_t a = As[i][k];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] += f.prod(a, Bs[k][s + 16 * q]);
+    if (++cnt == sb) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = f.reduce(acc[q]);  // counts as one product from here on
+      cnt = 1;
+    }
+  }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int j = s + 16 * q;
-    u128 acc = 0;
-    uint64_t cnt = 0;
-    for (int k = 0; k < kPanel; ++k) {
-      acc += f.prod(As[i][k], Bs[k][j]);
-      if (++cnt == sb) {
-        acc = f.reduce(acc);  // counts as one product from here on
-        cnt = 1;
-      }
-    }
-    uint64_t v = f.reduce(acc);
+    uint64_t v = f.reduce(acc[q]);
     if (negate && v) v = p - v;
     if (D) v = f.add(v, D[(int64_t)i * ldd + j]);
     Cout[(int64_t)i * ldc + j] = v;
