@@ -169,10 +169,20 @@ static bool use_tc(const RankRun& R) {
   return R.n >= R.ctx->tune.tc_cross[limb_class(R.fp->p)];
 }
 
+// Whatever path leaves rank_impl (an error included), the look-ahead work on
+// the second stream has finished before the workspaces it uses are reused.
+struct AuxDrain {
+  Ctx* C;
+  ~AuxDrain() {
+    if (C->aux) cudaStreamSynchronize(C->aux);
+  }
+};
+
 template <class F>
 static int rank_impl(const RankRun& R, size_t* rank_out) {
   const F f(*R.fp);
   Ctx* C = R.ctx;
+  AuxDrain drain{C};
   const int n = R.n;
   const int64_t ld = n;
   cudaStream_t st = R.st;
