@@ -165,6 +165,27 @@ int modlin_lc_batch(const modlin_job *jobs, size_t count, size_t *lcs_out);
 int modlin_lc_batch_device(const uint64_t *p, const uint64_t *const *d_data, const size_t *n,
                            size_t count, size_t *lcs_out, void *stream);
 
+/* Batch plans: the device job table of a batch of device-resident matrices
+ * (sides up to 8192) or sequences is built once; each launch then queues one
+ * counter reset and one persistent kernel on `stream`, with no allocation and
+ * no host synchronisation, so it can be captured in a CUDA graph and replayed
+ * (each launch clobbers the matrices, like modlin_rank_device: restore them
+ * between replays). Result i (rank or linear complexity of job i) is written
+ * to the caller's device array d_*_out[i] by each launch. Inputs and outputs
+ * must stay at the same addresses for the plan's life. No reference
+ * counterpart: the reference runs `reps` one after another (src/main.rs:82,
+ * :152). */
+typedef struct modlin_rank_batch_plan modlin_rank_batch_plan;
+typedef struct modlin_lc_batch_plan modlin_lc_batch_plan;
+int modlin_rank_batch_plan_new(const uint64_t *p, uint64_t *const *d_m, const size_t *n, size_t count,
+                               int64_t *d_ranks_out, modlin_rank_batch_plan **plan_out);
+int modlin_rank_batch_plan_launch(modlin_rank_batch_plan *plan, void *stream);
+void modlin_rank_batch_plan_free(modlin_rank_batch_plan *plan);
+int modlin_lc_batch_plan_new(const uint64_t *p, const uint64_t *const *d_s, const size_t *n, size_t count,
+                             int64_t *d_lcs_out, modlin_lc_batch_plan **plan_out);
+int modlin_lc_batch_plan_launch(modlin_lc_batch_plan *plan, void *stream);
+void modlin_lc_batch_plan_free(modlin_lc_batch_plan *plan);
+
 /* ---- p-values (src/stats.rs) -------------------------------------------- */
 
 double modlin_corank_prob(uint64_t p, size_t n, size_t d);          /* src/stats.rs:52-62 */

@@ -433,20 +433,28 @@ cudaError_t launch_bm_block(const BmJob& job, uint64_t* gws, int64_t smem_words,
   return cudaGetLastError();
 }
 
+// The batch kernel's dynamic shared memory cap is set once to the largest
+// size any batch asks for (200 KiB), so launches of any batch, graph-captured
+// ones included, need no attribute call.
+static cudaError_t bm_batch_attr() {
+  static cudaError_t e =
+      cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return e;
+}
+
 cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long long* d_next, uint64_t* gws,
                             int64_t gws_words, int64_t smem_words, int blocks, int threads, int64_t* d_out,
                             cudaStream_t st) {
   const size_t smem = (size_t)smem_words * 8;
-  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
-    cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = bm_batch_attr();
+  if (e != cudaSuccess) return e;
   bm_batch_kernel<<<blocks, threads, smem, st>>>(d_jobs, count, d_next, gws, gws_words, smem_words, d_out);
   return cudaGetLastError();
 }
 
 int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words) {
   const size_t smem = (size_t)smem_words * 8;
-  if (smem > 0)  // dynamic + static shared memory may pass 48 KiB even when smem alone does not
-    cudaFuncSetAttribute(bm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (bm_batch_attr() != cudaSuccess) return 0;
   int nb = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bm_batch_kernel, threads, smem);
   return nb;

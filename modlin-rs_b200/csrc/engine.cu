@@ -1394,6 +1394,128 @@ double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
 
 double modlin_last_trailing_macs(void) { return g_last_trailing_macs; }
 
+// ---- Batch plans: device state built once, launches that can be captured.
+}  // extern "C"
+
+struct modlin_rank_batch_plan {
+  int device;
+  int64_t count, maxn;
+  int blocks;
+  int64_t* out;  // caller's device array
+  modlin::DevBuf jobs, next;
+};
+
+struct modlin_lc_batch_plan {
+  int device;
+  int64_t count, smem_words, gws_words;
+  int blocks, threads;
+  int64_t* out;  // caller's device array
+  modlin::DevBuf jobs, next, gws;
+};
+
+extern "C" {
+
+int modlin_rank_batch_plan_new(const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
+                               int64_t* d_ranks_out, modlin_rank_batch_plan** plan_out) {
+  if (!plan_out || (count && (!p || !d_m || !n || !d_ranks_out))) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::vector<RankJob> jobs;
+  int64_t maxn = 1;
+  for (size_t i = 0; i < count; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    if ((int64_t)n[i] > kRankBatchMaxN) return MODLIN_EINVAL_N;
+    if (n[i] && !d_m[i]) return MODLIN_EINVAL_ARG;
+    jobs.push_back(RankJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_m[i], (int64_t)n[i], (int64_t)i});
+    maxn = std::max<int64_t>(maxn, (int64_t)n[i]);
+  }
+  std::stable_sort(jobs.begin(), jobs.end(), [](const RankJob& a, const RankJob& b) { return a.n > b.n; });
+  std::unique_ptr<modlin_rank_batch_plan> P(new modlin_rank_batch_plan());
+  P->device = C->device;
+  P->count = (int64_t)count;
+  P->maxn = maxn;
+  P->out = d_ranks_out;
+  const int per_sm = rank_batch_blocks_per_sm(maxn);
+  if (per_sm < 1) return MODLIN_ECUDA;
+  P->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * per_sm, (int64_t)count));
+  CK(P->jobs.ensure(std::max<size_t>(jobs.size(), 1) * sizeof(RankJob)));
+  CK(P->next.ensure(sizeof(unsigned long long)));
+  if (count) CK(cudaMemcpy(P->jobs.p, jobs.data(), jobs.size() * sizeof(RankJob), cudaMemcpyHostToDevice));
+  *plan_out = P.release();
+  return MODLIN_OK;
+}
+
+int modlin_rank_batch_plan_launch(modlin_rank_batch_plan* P, void* stream) {
+  if (!P) return MODLIN_EINVAL_ARG;
+  if (P->count == 0) return MODLIN_OK;
+  CK(launch_rank_batch(P->jobs.as<RankJob>(), P->count, P->next.as<unsigned long long>(), P->maxn, P->blocks,
+                       P->out, user_stream(stream)));
+  g_launches += 2;
+  return MODLIN_OK;
+}
+
+void modlin_rank_batch_plan_free(modlin_rank_batch_plan* P) {
+  if (!P) return;
+  cudaFree(P->jobs.p);
+  cudaFree(P->next.p);
+  delete P;
+}
+
+int modlin_lc_batch_plan_new(const uint64_t* p, const uint64_t* const* d_s, const size_t* n, size_t count,
+                             int64_t* d_lcs_out, modlin_lc_batch_plan** plan_out) {
+  if (!plan_out || (count && (!p || !d_s || !n || !d_lcs_out))) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::vector<BmJob> jobs;
+  int64_t maxn = 1;
+  for (size_t i = 0; i < count; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    if (n[i] && !d_s[i]) return MODLIN_EINVAL_ARG;
+    if (n[i] > (size_t)1 << 30) return MODLIN_EINVAL_N;
+    jobs.push_back(BmJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_s[i], (int64_t)n[i], (int64_t)i});
+    maxn = std::max<int64_t>(maxn, (int64_t)n[i]);
+  }
+  std::stable_sort(jobs.begin(), jobs.end(), [](const BmJob& a, const BmJob& b) { return a.n > b.n; });
+  std::unique_ptr<modlin_lc_batch_plan> P(new modlin_lc_batch_plan());
+  P->device = C->device;
+  P->count = (int64_t)count;
+  P->out = d_lcs_out;
+  P->threads = C->tune.bm_batch_threads[bm_batch_class(maxn)];
+  P->smem_words = std::min<int64_t>(3 * maxn, (200 * 1024) / 8);
+  const int per_sm = std::max(1, bm_batch_max_blocks_per_sm(P->threads, P->smem_words));
+  P->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * per_sm, (int64_t)count));
+  P->gws_words = 3 * maxn > P->smem_words ? 3 * maxn : 0;
+  CK(P->jobs.ensure(std::max<size_t>(jobs.size(), 1) * sizeof(BmJob)));
+  CK(P->next.ensure(sizeof(unsigned long long)));
+  if (P->gws_words) CK(P->gws.ensure((size_t)P->blocks * P->gws_words * 8));
+  if (count) CK(cudaMemcpy(P->jobs.p, jobs.data(), jobs.size() * sizeof(BmJob), cudaMemcpyHostToDevice));
+  *plan_out = P.release();
+  return MODLIN_OK;
+}
+
+int modlin_lc_batch_plan_launch(modlin_lc_batch_plan* P, void* stream) {
+  if (!P) return MODLIN_EINVAL_ARG;
+  if (P->count == 0) return MODLIN_OK;
+  cudaStream_t st = user_stream(stream);
+  CK(cudaMemsetAsync(P->next.p, 0, sizeof(unsigned long long), st));
+  CK(launch_bm_batch(P->jobs.as<BmJob>(), P->count, P->next.as<unsigned long long>(), P->gws.as<uint64_t>(),
+                     P->gws_words, P->smem_words, P->blocks, P->threads, P->out, st));
+  g_launches += 2;
+  return MODLIN_OK;
+}
+
+void modlin_lc_batch_plan_free(modlin_lc_batch_plan* P) {
+  if (!P) return;
+  cudaFree(P->jobs.p);
+  cudaFree(P->next.p);
+  cudaFree(P->gws.p);
+  delete P;
+}
+
 int modlin_autotune(char* report, size_t cap) {
   Ctx* C = nullptr;
   int rc = get_ctx(&C);

@@ -219,9 +219,19 @@ __global__ void __launch_bounds__(kT, 2)
 
 size_t rank_batch_smem_bytes(int64_t max_n) { return sizeof(BatchSmem) + (size_t)max_n * sizeof(int); }
 
+// The kernel's dynamic shared memory cap is set once to what the largest
+// side needs, so launches of any batch (graph-captured ones included) need no
+// attribute call.
+static cudaError_t rank_batch_attr() {
+  static cudaError_t e =
+      cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)rank_batch_smem_bytes(kRankBatchMaxN));
+  return e;
+}
+
 int rank_batch_blocks_per_sm(int64_t max_n) {
   const size_t smem = rank_batch_smem_bytes(max_n);
-  cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (rank_batch_attr() != cudaSuccess) return 0;
   int nb = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rank_batch_kernel, kT, smem);
   return nb;
@@ -230,7 +240,7 @@ int rank_batch_blocks_per_sm(int64_t max_n) {
 cudaError_t launch_rank_batch(const RankJob* d_jobs, int64_t count, unsigned long long* d_next, int64_t max_n,
                               int blocks, int64_t* d_out, cudaStream_t st) {
   const size_t smem = rank_batch_smem_bytes(max_n);
-  cudaError_t e = cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = rank_batch_attr();
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;

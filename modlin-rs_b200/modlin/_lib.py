@@ -97,6 +97,11 @@ def lib():
     _proto(L, "modlin_last_trailing_ms", ctypes.c_double, [])
     _proto(L, "modlin_last_trailing_macs", ctypes.c_double, [])
     _proto(L, "modlin_autotune", ci, [ctypes.c_char_p, szt])
+    for kind in ("rank", "lc"):
+        _proto(L, f"modlin_{kind}_batch_plan_new", ci, [u64p, ctypes.POINTER(vp), sztp, szt, vp,
+                                                        ctypes.POINTER(vp)])
+        _proto(L, f"modlin_{kind}_batch_plan_launch", ci, [vp, vp])
+        _proto(L, f"modlin_{kind}_batch_plan_free", None, [vp])
     _lib = L
     return L
 
@@ -118,4 +123,6 @@ EXPORTED = [
     "modlin_gen_uniform", "modlin_gen_uniform_device", "modlin_gen_planted", "modlin_reduce_device",
     "modlin_gen_planted_device", "modlin_gen_planted_batch_device",
     "modlin_kernel_launches", "modlin_last_trailing_ms", "modlin_last_trailing_macs", "modlin_autotune",
+    "modlin_rank_batch_plan_new", "modlin_rank_batch_plan_launch", "modlin_rank_batch_plan_free",
+    "modlin_lc_batch_plan_new", "modlin_lc_batch_plan_launch", "modlin_lc_batch_plan_free",
 ]

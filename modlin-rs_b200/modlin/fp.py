@@ -166,3 +166,35 @@ def trailing_update_device(field, c_ptr: int, ldc: int, M: int, N: int, l_ptr: i
     rc = lib().modlin_trailing_update_device(_p(field), c_ptr, ldc, M, N, l_ptr, u_ptr, ldu, K, KERNELS[kernel],
                                              stream or None)
     check(rc, "trailing_update_device")
+
+
+class BatchPlan:
+    """A device batch of ranks (kind "rank") or linear complexities ("lc"):
+    built once, then launched asynchronously (capturable in a CUDA graph) any
+    number of times; every launch writes job i's result to the device int64
+    array at `out_ptr` (slot i)."""
+
+    def __init__(self, kind: str, ps, ptrs, ns, out_ptr: int):
+        self.kind, self.count = kind, len(ptrs)
+        k = self.count
+        P = (ctypes.c_uint64 * max(k, 1))(*ps)
+        D = (ctypes.c_void_p * max(k, 1))(*ptrs)
+        N = (szt * max(k, 1))(*ns)
+        h = ctypes.c_void_p()
+        rc = getattr(lib(), f"modlin_{kind}_batch_plan_new")(P, D, N, k, out_ptr, ctypes.byref(h))
+        check(rc, f"{kind}_batch_plan_new")
+        self._h = h
+
+    def launch(self, stream: int = 0) -> None:
+        check(getattr(lib(), f"modlin_{self.kind}_batch_plan_launch")(self._h, stream or None), "plan_launch")
+
+    def free(self) -> None:
+        if getattr(self, "_h", None):
+            getattr(lib(), f"modlin_{self.kind}_batch_plan_free")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
