@@ -302,6 +302,29 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     batch["plain_one_per_launch"] = {"sequences": len(idx), "steps": sub, "ms": pms,
                                      "steps_per_s": sub / (pms * 1e-3)}
     batch["speedup_vs_plain"] = batch["steps_per_s"] / batch["plain_one_per_launch"]["steps_per_s"]
+    # The batch as a plan captured in a CUDA graph (one counter reset and one
+    # persistent launch per replay).
+    out = torch.empty(len(jobs), dtype=torch.int64, device="cuda")
+    plan = mfp.BatchPlan("lc", ps, ptrs, ns, out.data_ptr())
+    g = torch.cuda.CUDAGraph()
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(cs):
+        with torch.cuda.graph(g, stream=cs):
+            plan.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.current_stream().wait_stream(cs)
+    g.replay()
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == lcs
+    e0.record()
+    for _ in range(steps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    gms = e0.elapsed_time(e1) / steps
+    batch["cuda_graph"] = {"ms": gms, "steps_per_s": total / (gms * 1e-3)}
+    del g
+    plan.free()
     if cpu:
         # The reference runs BM single-threaded, one sequence after another.
         import oracle
@@ -430,6 +453,31 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
            "non_generic_ranks_equal_to_oracle": confirmed,
            "step": "restore the 4096 matrices from a pristine copy + one batched call"}
     assert confirmed == len(mism)
+    # The same batch as a plan captured in a CUDA graph: each replay restores
+    # the matrices and ranks them all (one copy, one counter reset, one
+    # persistent launch; no host synchronisation inside).
+    out = torch.empty(len(jobs), dtype=torch.int64, device="cuda")
+    plan = mfp.BatchPlan("rank", ps, ptrs, ns, out.data_ptr())
+    g = torch.cuda.CUDAGraph()
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(cs):
+        with torch.cuda.graph(g, stream=cs):
+            work.copy_(pristine)
+            plan.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.current_stream().wait_stream(cs)
+    g.replay()
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == ranks
+    e0.record()
+    for _ in range(steps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    gms = e0.elapsed_time(e1) / steps
+    res["cuda_graph"] = {"ms": gms, "modmac_per_s": work_mac / (gms * 1e-3), "matrices_per_s": len(jobs) / (gms * 1e-3)}
+    del g
+    plan.free()
     # The same matrices through the single-matrix engine, one call each.
     idx = list(range(0, len(jobs), max(1, len(jobs) // single_sample)))[:single_sample]
     work.copy_(pristine)
