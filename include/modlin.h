@@ -158,6 +158,11 @@ int modlin_rank_batch(const modlin_job *jobs, size_t count, size_t *ranks_out);
  * into one persistent launch; larger ones run one after another. */
 int modlin_rank_batch_device(const uint64_t *p, uint64_t *const *d_m, const size_t *n, size_t count,
                              size_t *ranks_out, void *stream);
+/* modlin_rank_batch_device with options: kernel MODLIN_RANK_TC puts every job
+ * of side up to 8192 on the tensor-core batch kernel, MODLIN_RANK_PLAIN on the
+ * integer-pipe one, MODLIN_RANK_AUTO splits them at the tuned side. */
+int modlin_rank_batch_device_ex(const uint64_t *p, uint64_t *const *d_m, const size_t *n, size_t count,
+                                const modlin_rank_opts *opts, size_t *ranks_out, void *stream);
 /* Linear complexities of `count` sequences in one persistent launch. */
 int modlin_lc_batch(const modlin_job *jobs, size_t count, size_t *lcs_out);
 

@@ -59,6 +59,7 @@ struct Tune {
   int bm_threads[4] = {256, 256, 1024, 1024};       // n < 1024, < 4096, < 16384, longer
   int bm_cluster_min = 16384;
   int bm_batch_threads[3] = {128, 256, 512};        // longest < 512, < 2048, longer
+  int batch_tc_min = 1 << 30;  // batched rank: sides on the tensor-core kernel (off until measured faster)
 };
 
 static int limb_class(uint64_t p) {
@@ -618,7 +619,8 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
 // Batched rank: jobs up to kRankBatchMaxN go into one persistent launch
 // (largest first), larger ones through the single-matrix engine afterwards.
 static int rank_batch_locked(Ctx* C, const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
-                             size_t* ranks_out, cudaStream_t st, std::unique_lock<std::mutex>& g) {
+                             size_t* ranks_out, cudaStream_t st, std::unique_lock<std::mutex>& g,
+                             int kernel = MODLIN_RANK_AUTO) {
   if (count == 0) return MODLIN_OK;
   std::vector<RankJob> jobs;
   std::vector<size_t> big;
@@ -639,21 +641,43 @@ static int rank_batch_locked(Ctx* C, const uint64_t* p, uint64_t* const* d_m, co
   }
   if (!jobs.empty()) {
     // Largest first (work ~ n^3): the persistent CTAs then finish together.
+    // Sides from the tuned threshold on go to the tensor-core kernel, the rest to
+    // the integer-pipe kernel, one launch each on the same stream.
     std::stable_sort(jobs.begin(), jobs.end(), [](const RankJob& a, const RankJob& b) { return a.n > b.n; });
+    const int64_t tc_min = kernel == MODLIN_RANK_TC ? 0 : kernel == MODLIN_RANK_PLAIN ? INT64_MAX
+                                                                                        : C->tune.batch_tc_min;
+    size_t ntc = 0;
+    while (ntc < jobs.size() && jobs[ntc].n >= tc_min) ++ntc;
     CK(C->rbjobs.ensure(sizeof(RankJob) * jobs.size()));
-    CK(C->bmnext.ensure(sizeof(unsigned long long)));
+    CK(C->bmnext.ensure(2 * sizeof(unsigned long long)));
     CK(C->rbout.ensure(sizeof(int64_t) * count));
+    CK(C->tcerr.ensure(2 * sizeof(int)));
+    CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
     CK(cudaMemcpyAsync(C->rbjobs.p, jobs.data(), sizeof(RankJob) * jobs.size(), cudaMemcpyHostToDevice, st));
-    int per_sm = rank_batch_blocks_per_sm(maxn);
-    if (per_sm < 1) return MODLIN_ECUDA;
-    int blocks = C->num_sms * per_sm;
-    if ((size_t)blocks > jobs.size()) blocks = (int)jobs.size();
-    CK(launch_rank_batch(C->rbjobs.as<RankJob>(), (int64_t)jobs.size(), C->bmnext.as<unsigned long long>(), maxn,
-                         blocks, C->rbout.as<int64_t>(), st));
-    g_launches += 2;
+    if (ntc > 0) {
+      const int per_sm = rank_batch_tc_blocks_per_sm(jobs[0].n);
+      if (per_sm < 1) return MODLIN_ECUDA;
+      const int blocks = (int)std::min<int64_t>((int64_t)C->num_sms * per_sm, (int64_t)ntc);
+      CK(launch_rank_batch_tc(C->rbjobs.as<RankJob>(), (int64_t)ntc, C->bmnext.as<unsigned long long>(), jobs[0].n,
+                              blocks, C->rbout.as<int64_t>(), C->tcerr.as<int>(), st));
+      g_launches += 2;
+    }
+    if (ntc < jobs.size()) {
+      const int64_t mx = jobs[ntc].n;
+      int per_sm = rank_batch_blocks_per_sm(mx);
+      if (per_sm < 1) return MODLIN_ECUDA;
+      int blocks = C->num_sms * per_sm;
+      if ((size_t)blocks > jobs.size() - ntc) blocks = (int)(jobs.size() - ntc);
+      CK(launch_rank_batch(C->rbjobs.as<RankJob>() + ntc, (int64_t)(jobs.size() - ntc),
+                           C->bmnext.as<unsigned long long>() + 1, mx, blocks, C->rbout.as<int64_t>(), st));
+      g_launches += 2;
+    }
     std::vector<int64_t> out(count);
     CK(cudaMemcpyAsync(out.data(), C->rbout.p, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, st));
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, C->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (err) return MODLIN_ETIMEOUT;
     for (const RankJob& j : jobs) ranks_out[j.slot] = (size_t)out[j.slot];
   }
   if (!big.empty()) {
@@ -818,7 +842,45 @@ static int autotune_locked(Ctx* C, std::string& rep) {
     rep += "}";
     T.two_panel_min = crossover(tsz, two_wins, 1 << 30);
   }
-  // 3. BM: threads per CTA of the block kernel by length class, then the
+  // 3. Batched rank: tensor-core kernel against the integer-pipe kernel, per
+  //    side (a batch of two matrices per SM, 2^61 - 1).
+  {
+    const std::vector<int> bsz = {128, 256, 512, 1024};
+    std::vector<bool> tc_wins;
+    const int cnt = 2 * C->num_sms;
+    rep += ", \"batch_tc_ms\": {";
+    const int saved = C->tune.batch_tc_min;
+    for (int n : bsz) {
+      const size_t nn = (size_t)n * n;
+      TK(C->tunebuf.ensure((size_t)cnt * nn * 8));
+      TK(C->batchm.ensure((size_t)cnt * nn * 8));
+      uint64_t nl = 0;
+      TK(gen_uniform_device(kM61, 31337 + n, C->tunebuf.as<uint64_t>(), (uint64_t)cnt * nn, st, &nl));
+      std::vector<uint64_t> ps(cnt, kM61);
+      std::vector<uint64_t*> ptrs(cnt);
+      std::vector<size_t> ns(cnt, (size_t)n), out(cnt);
+      for (int i = 0; i < cnt; ++i) ptrs[i] = C->batchm.as<uint64_t>() + (size_t)i * nn;
+      float t[2];
+      for (int k = 0; k < 2; ++k) {
+        C->tune.batch_tc_min = k == 0 ? (1 << 30) : 0;
+        std::unique_lock<std::mutex> dummy;  // the context lock is already held by the caller
+        t[k] = best_ms(C, 2, [&]() -> int {
+          if (cudaMemcpyAsync(C->batchm.p, C->tunebuf.p, (size_t)cnt * nn * 8, cudaMemcpyDeviceToDevice, st) !=
+              cudaSuccess)
+            return MODLIN_ECUDA;
+          return rank_batch_locked(C, ps.data(), ptrs.data(), ns.data(), cnt, out.data(), st, dummy);
+        }, &rc);
+        C->tune.batch_tc_min = saved;
+        if (rc) return rc;
+      }
+      tc_wins.push_back(t[1] <= t[0]);
+      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == bsz[0] ? "" : ", ", n, t[0], t[1]);
+      rep += buf;
+    }
+    rep += "}";
+    T.batch_tc_min = crossover(bsz, tc_wins, 1 << 30);
+  }
+  // 4. BM: threads per CTA of the block kernel by length class, then the
   //    block/cluster crossover.
   FieldParams fp;
   make_field_params(kM61, &fp);
@@ -883,7 +945,7 @@ static int autotune_locked(Ctx* C, std::string& rep) {
     T.bm_cluster_min = crossover(csz, cl_wins, 1 << 30);
   }
   rep += "}";
-  // 4. BM batches: threads per CTA by the longest sequence.
+  // 5. BM batches: threads per CTA by the longest sequence.
   {
     const int64_t lo[3] = {64, 512, 2048}, hi[3] = {512, 2048, 8192};
     const int bthr[3] = {128, 256, 512};
@@ -931,10 +993,11 @@ static int autotune_locked(Ctx* C, std::string& rep) {
   C->tune = T;
   std::snprintf(buf, sizeof buf,
                 ", \"choice\": {\"tc_crossover\": [%d, %d, %d, %d], \"two_panel_min\": %d, "
-                "\"bm_threads\": [%d, %d, %d, %d], \"bm_cluster_min\": %d, \"bm_batch_threads\": [%d, %d, %d]}}",
-                T.tc_cross[0], T.tc_cross[1], T.tc_cross[2], T.tc_cross[3], T.two_panel_min, T.bm_threads[0],
-                T.bm_threads[1], T.bm_threads[2], T.bm_threads[3], T.bm_cluster_min, T.bm_batch_threads[0],
-                T.bm_batch_threads[1], T.bm_batch_threads[2]);
+                "\"batch_tc_min\": %d, \"bm_threads\": [%d, %d, %d, %d], \"bm_cluster_min\": %d, "
+                "\"bm_batch_threads\": [%d, %d, %d]}}",
+                T.tc_cross[0], T.tc_cross[1], T.tc_cross[2], T.tc_cross[3], T.two_panel_min, T.batch_tc_min,
+                T.bm_threads[0], T.bm_threads[1], T.bm_threads[2], T.bm_threads[3], T.bm_cluster_min,
+                T.bm_batch_threads[0], T.bm_batch_threads[1], T.bm_batch_threads[2]);
   rep += buf;
   return MODLIN_OK;
 }
@@ -1128,6 +1191,23 @@ int modlin_lc_batch(const modlin_job* jobs, size_t count, size_t* lcs_out) {
     off += jobs[i].n;
   }
   return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, lcs_out, C->stream);
+}
+
+int modlin_rank_batch_device_ex(const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
+                                const modlin_rank_opts* opts, size_t* ranks_out, void* stream) {
+  if (count && (!p || !d_m || !n || !ranks_out)) return MODLIN_EINVAL_ARG;
+  for (size_t i = 0; i < count; ++i) {
+    FieldParams fp;
+    if (!make_field_params(p[i], &fp)) return MODLIN_EINVAL_P;
+    if (n[i] && !d_m[i]) return MODLIN_EINVAL_ARG;
+    if (n[i] > (size_t)INT32_MAX / 2) return MODLIN_EINVAL_N;
+  }
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::unique_lock<std::mutex> g(C->mu);
+  return rank_batch_locked(C, p, d_m, n, count, ranks_out, user_stream(stream), g,
+                           opts ? opts->kernel : MODLIN_RANK_AUTO);
 }
 
 int modlin_rank_batch_device(const uint64_t* p, uint64_t* const* d_m, const size_t* n, size_t count,
@@ -1399,10 +1479,11 @@ double modlin_last_trailing_macs(void) { return g_last_trailing_macs; }
 
 struct modlin_rank_batch_plan {
   int device;
-  int64_t count, maxn;
-  int blocks;
+  int64_t count, ntc;      // jobs, of which the first ntc (largest) on the tensor cores
+  int64_t max_tc, max_small;
+  int blocks_tc, blocks_small;
   int64_t* out;  // caller's device array
-  modlin::DevBuf jobs, next;
+  modlin::DevBuf jobs, next, err;
 };
 
 struct modlin_lc_batch_plan {
@@ -1431,17 +1512,24 @@ int modlin_rank_batch_plan_new(const uint64_t* p, uint64_t* const* d_m, const si
     jobs.push_back(RankJob{fp.p, fp.mu_lo, fp.mu_hi, fp.safe_batch, d_m[i], (int64_t)n[i], (int64_t)i});
     maxn = std::max<int64_t>(maxn, (int64_t)n[i]);
   }
+  (void)maxn;
   std::stable_sort(jobs.begin(), jobs.end(), [](const RankJob& a, const RankJob& b) { return a.n > b.n; });
   std::unique_ptr<modlin_rank_batch_plan> P(new modlin_rank_batch_plan());
   P->device = C->device;
   P->count = (int64_t)count;
-  P->maxn = maxn;
   P->out = d_ranks_out;
-  const int per_sm = rank_batch_blocks_per_sm(maxn);
-  if (per_sm < 1) return MODLIN_ECUDA;
-  P->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * per_sm, (int64_t)count));
+  P->ntc = 0;
+  while (P->ntc < (int64_t)jobs.size() && jobs[P->ntc].n >= C->tune.batch_tc_min) ++P->ntc;
+  P->max_tc = P->ntc ? jobs[0].n : 1;
+  P->max_small = P->ntc < (int64_t)jobs.size() ? jobs[P->ntc].n : 1;
+  const int ptc = rank_batch_tc_blocks_per_sm(P->max_tc), psm = rank_batch_blocks_per_sm(P->max_small);
+  if (ptc < 1 || psm < 1) return MODLIN_ECUDA;
+  P->blocks_tc = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * ptc, P->ntc));
+  P->blocks_small =
+      (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * psm, (int64_t)count - P->ntc));
   CK(P->jobs.ensure(std::max<size_t>(jobs.size(), 1) * sizeof(RankJob)));
-  CK(P->next.ensure(sizeof(unsigned long long)));
+  CK(P->next.ensure(2 * sizeof(unsigned long long)));
+  CK(P->err.ensure(2 * sizeof(int)));
   if (count) CK(cudaMemcpy(P->jobs.p, jobs.data(), jobs.size() * sizeof(RankJob), cudaMemcpyHostToDevice));
   *plan_out = P.release();
   return MODLIN_OK;
@@ -1450,9 +1538,17 @@ int modlin_rank_batch_plan_new(const uint64_t* p, uint64_t* const* d_m, const si
 int modlin_rank_batch_plan_launch(modlin_rank_batch_plan* P, void* stream) {
   if (!P) return MODLIN_EINVAL_ARG;
   if (P->count == 0) return MODLIN_OK;
-  CK(launch_rank_batch(P->jobs.as<RankJob>(), P->count, P->next.as<unsigned long long>(), P->maxn, P->blocks,
-                       P->out, user_stream(stream)));
-  g_launches += 2;
+  cudaStream_t st = user_stream(stream);
+  // -1 marks a job whose rank was not written (a bounded wait expired).
+  CK(cudaMemsetAsync(P->out, 0xff, (size_t)P->count * sizeof(int64_t), st));
+  CK(cudaMemsetAsync(P->err.p, 0, 2 * sizeof(int), st));
+  if (P->ntc > 0)
+    CK(launch_rank_batch_tc(P->jobs.as<RankJob>(), P->ntc, P->next.as<unsigned long long>(), P->max_tc, P->blocks_tc,
+                            P->out, P->err.as<int>(), st));
+  if (P->ntc < P->count)
+    CK(launch_rank_batch(P->jobs.as<RankJob>() + P->ntc, P->count - P->ntc, P->next.as<unsigned long long>() + 1,
+                         P->max_small, P->blocks_small, P->out, st));
+  g_launches += 4;
   return MODLIN_OK;
 }
 
@@ -1460,6 +1556,7 @@ void modlin_rank_batch_plan_free(modlin_rank_batch_plan* P) {
   if (!P) return;
   cudaFree(P->jobs.p);
   cudaFree(P->next.p);
+  cudaFree(P->err.p);
   delete P;
 }
 

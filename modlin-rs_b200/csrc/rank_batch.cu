@@ -223,9 +223,11 @@ size_t rank_batch_smem_bytes(int64_t max_n) { return sizeof(BatchSmem) + (size_t
 // side needs, so launches of any batch (graph-captured ones included) need no
 // attribute call.
 static cudaError_t rank_batch_attr() {
-  static cudaError_t e =
-      cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)rank_batch_smem_bytes(kRankBatchMaxN));
+  static cudaError_t e = [] {
+    cudaError_t r = cudaFuncSetAttribute(rank_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)rank_batch_smem_bytes(kRankBatchMaxN));
+    return r;
+  }();
   return e;
 }
 

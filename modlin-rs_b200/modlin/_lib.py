@@ -79,6 +79,8 @@ def lib():
     _proto(L, "modlin_rank_batch", ci, [ctypes.POINTER(Job), szt, sztp])
     _proto(L, "modlin_lc_batch", ci, [ctypes.POINTER(Job), szt, sztp])
     _proto(L, "modlin_rank_batch_device", ci, [u64p, ctypes.POINTER(vp), sztp, szt, sztp, vp])
+    _proto(L, "modlin_rank_batch_device_ex", ci, [u64p, ctypes.POINTER(vp), sztp, szt, ctypes.POINTER(RankOpts),
+                                                  sztp, vp])
     _proto(L, "modlin_lc_batch_device", ci, [u64p, ctypes.POINTER(vp), sztp, szt, sztp, vp])
     for name in ("modlin_corank_prob", "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue"):
         _proto(L, name, ctypes.c_double, [u64, szt, szt])
@@ -117,7 +119,7 @@ EXPORTED = [
     "modlin_field_mul", "modlin_rank", "modlin_rank_ex", "modlin_rank_device", "modlin_trailing_update_device",
     "modlin_linear_complexity", "modlin_linear_complexity_ex", "modlin_linear_complexity_device",
     "modlin_linear_complexity_device_noalloc",
-    "modlin_rank_batch", "modlin_rank_batch_device", "modlin_lc_batch", "modlin_lc_batch_device", "modlin_corank_prob",
+    "modlin_rank_batch", "modlin_rank_batch_device", "modlin_rank_batch_device_ex", "modlin_lc_batch", "modlin_lc_batch_device", "modlin_corank_prob",
     "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue", "modlin_pretty_p_value",
     "modlin_prng_new", "modlin_prng_name", "modlin_prng_fill", "modlin_prng_free",
     "modlin_gen_uniform", "modlin_gen_uniform_device", "modlin_gen_planted", "modlin_reduce_device",

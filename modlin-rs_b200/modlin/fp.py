@@ -127,15 +127,18 @@ def rank_batch(items) -> list[int]:
     return [int(out[i]) for i in range(len(arrs))]
 
 
-def rank_batch_device(ps, ptrs, ns, stream: int = 0) -> list[int]:
+def rank_batch_device(ps, ptrs, ns, stream: int = 0, kernel: str = "auto") -> list[int]:
     """Device-resident batch: ``ptrs[i]`` points at an ``ns[i]`` x ``ns[i]``
-    matrix mod ``ps[i]`` (clobbered)."""
+    matrix mod ``ps[i]`` (clobbered). ``kernel``: "auto" (tuned split),
+    "tc" (tensor-core batch kernel) or "plain"."""
     k = len(ptrs)
-    P = (ctypes.c_uint64 * k)(*ps)
-    D = (ctypes.c_void_p * k)(*ptrs)
-    N = (szt * k)(*ns)
-    out = (szt * k)()
-    check(lib().modlin_rank_batch_device(P, D, N, k, out, stream or None), "rank_batch_device")
+    P = (ctypes.c_uint64 * max(k, 1))(*ps)
+    D = (ctypes.c_void_p * max(k, 1))(*ptrs)
+    N = (szt * max(k, 1))(*ns)
+    out = (szt * max(k, 1))()
+    opts = RankOpts(KERNELS[kernel], 0)
+    check(lib().modlin_rank_batch_device_ex(P, D, N, k, ctypes.byref(opts), out, stream or None),
+          "rank_batch_device")
     return [int(out[i]) for i in range(k)]
 
 

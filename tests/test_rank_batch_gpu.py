@@ -80,3 +80,23 @@ def test_batch_device_matches_host_form(M):
 def test_batch_empty_and_zero_side(M):
     assert M.rank_batch([]) == []
     assert M.rank_batch([(M61, np.zeros(0, dtype=np.uint64)), (M61, np.eye(2, dtype=np.uint64))]) == [0, 2]
+
+
+def test_batch_tensor_core_variant_matches_oracle(M, O):
+    """The tensor-core batch kernel (one CTA per matrix, trailing updates as
+    limb GEMMs on its SM), forced for every job, on every limb count: the
+    oracle's ranks, as the integer-pipe kernel's."""
+    import torch
+    rng = np.random.default_rng(77)
+    items = []
+    for i in range(42):
+        p = PRIMES[i % len(PRIMES)]
+        n = int(rng.integers(1, 420))
+        a = M.gen.uniform(p, 300 + i, n * n) if i % 2 else M.gen.planted(p, max(1, n // 2), 300 + i, n * n)
+        items.append((p, n, a))
+    want = [O.rank(p, a, n) for p, n, a in items]
+    for kernel in ("tc", "plain"):
+        bufs = [torch.from_numpy(a.view(np.int64).copy()).cuda() for _, _, a in items]
+        got = M.fp.rank_batch_device([p for p, _, _ in items], [b.data_ptr() for b in bufs],
+                                     [n for _, n, _ in items], kernel=kernel)
+        assert got == want, kernel
