@@ -161,7 +161,7 @@ struct RankRun {
   std::vector<int>* pcols;
   modlin_progress_fn cb;
   void* cb_ctx;
-  int two_panel_min;  // smallest side for two-panel steps (tensor-core path)
+  int two_panel_min;  // smallest remaining block (rows) for two-panel steps (tensor-core path)
 };
 
 static bool use_tc(const RankRun& R) {
@@ -283,7 +283,9 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     const int jend = std::min(col + kPanel, n);
     const int W = jend - col;
     const int r0 = rank;
-    if (tc && n >= R.two_panel_min && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
+    // Two-panel steps while the remaining block is at least two_panel_min
+    // rows (below that, one-panel steps have the shorter block chain).
+    if (tc && n - r0 >= R.two_panel_min && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
       // Two-panel block step: P = A[r0 .. r0+128, col .. col+128) split into
       // 64 x 64 blocks [P11 P12; P21 P22]. With V11 = P11^-1 and the Schur
       // complement S = P22 - P21 V11 P12 invertible, the multipliers of the
@@ -330,7 +332,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
             auto evp = take_events();
             cudaEventRecord(evp.first, st);
             CK(tc_split_a(*R.fp, Hb, H0, r0, rb, n, 2 * kPanel, tA, st));
-            const bool ahead = c2 + 2 * kPanel <= n && n - rb >= 2 * kPanel;
+            const bool ahead = c2 + 2 * kPanel <= n && n - rb >= 2 * kPanel && n - rb >= R.two_panel_min;
             int cw = c2;
             if (ahead) {
               // The next step's 128 columns first; its blocks on the second
