@@ -46,6 +46,8 @@ extern "C" {
  * complexity); replaces the reference's generic `pl: &mut impl ProgressLog`
  * (src/fp.rs:125, :260), which has no C form. May be NULL. */
 typedef void (*modlin_progress_fn)(void *ctx, size_t done, size_t total);
+/* A generator under test (src/prng.rs); see the generator section below. */
+typedef struct modlin_prng modlin_prng;
 
 /* Human-readable text for a return code. */
 const char *modlin_strerror(int code);
@@ -95,6 +97,11 @@ int modlin_rank_ex(uint64_t p, uint64_t *m, size_t n, const modlin_rank_opts *op
  * (NULL = legacy default stream). The call returns when the rank is known. */
 int modlin_rank_device(uint64_t p, uint64_t *d_m, size_t n, const modlin_rank_opts *opts,
                        size_t *rank_out, size_t *pivot_cols_out, void *stream);
+/* One matrix of the -R test (src/main.rs:94-112): the next n*n outputs of g,
+ * reduced mod p, row by row, generated in device memory
+ * (modlin_prng_fill_device) and ranked there; g advances past them. */
+int modlin_rank_prng(uint64_t p, modlin_prng *g, size_t n, const modlin_rank_opts *opts, size_t *rank_out,
+                     modlin_progress_fn cb, void *cb_ctx);
 
 /* The trailing update of one panel (src/fp.rs:202-248) as a standalone
  * device operation: C[M x N] -= L[M x K] * U[K x N] (mod p), all entries in
@@ -207,7 +214,6 @@ int modlin_pretty_p_value(double p, char *buf, size_t cap);
 #define MODLIN_PRNG_MIXMAX240 240
 #define MODLIN_PRNG_MIXMAX256 256
 
-typedef struct modlin_prng modlin_prng;
 /* Prng::try_new (src/prng.rs:58, :152): NULL + *err = MODLIN_EINVAL_ARG for
  * a rejected seed (MIXMAX forbids 0) or an unknown kind. */
 modlin_prng *modlin_prng_new(int kind, uint64_t seed, int *err);
@@ -216,6 +222,21 @@ const char *modlin_prng_name(int kind);
 /* count successive next_u64() outputs. */
 void modlin_prng_fill(modlin_prng *g, uint64_t *out, size_t count);
 void modlin_prng_free(modlin_prng *g);
+/* The same `count` outputs, written to device memory by many warps at once
+ * from jump-ahead states (no reference counterpart: the reference fills its
+ * matrix one next_u64() at a time, src/main.rs:94-104). Bit-identical to
+ * modlin_prng_fill; each output is reduced mod p (Field::reduce) unless p is
+ * 0. g advances past the outputs, so host and device fills interleave.
+ * Returns after the fill is complete. */
+int modlin_prng_fill_device(modlin_prng *g, uint64_t p, uint64_t *d_out, size_t count, void *stream);
+/* A generator's position as 64-bit words, to save and restore it:
+ * xoroshiro128++ 2 words (s0, s1); MIXMAX-N N + 2 words (v[0..N), sumtot,
+ * counter). set_state rejects (MODLIN_EINVAL_ARG) a wrong word count, a
+ * MIXMAX entry above 2^61 - 1 (no step produces one) or a counter outside
+ * [1, N]. */
+size_t modlin_prng_state_words(int kind);
+int modlin_prng_get_state(const modlin_prng *g, uint64_t *words, size_t n);
+int modlin_prng_set_state(modlin_prng *g, const uint64_t *words, size_t n);
 
 /* ---- Synthetic workloads ------------------------------------------------ */
 

@@ -17,6 +17,7 @@
 #include "bm_kernels.cuh"
 #include "field.cuh"
 #include "gen_kernels.cuh"
+#include "prng_kernels.cuh"
 #include "rank_batch.cuh"
 #include "rank_kernels.cuh"
 #include "rank_tc.cuh"
@@ -91,6 +92,7 @@ struct Ctx {
   DevBuf jump;           // jump-ahead scratch of the long planted generator
   DevBuf batchm, rbjobs, rbout;  // batched rank: matrix arena, jobs, ranks
   DevBuf tunebuf;                // autotuner inputs
+  PrngCache prng;                // generator fills: jump matrices, workspace
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
 };
@@ -1468,6 +1470,39 @@ int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) 
   CK(reduce_device(fp, d_x, count, st));
   g_launches++;
   return cuda_rc(cudaStreamSynchronize(st));
+}
+
+int modlin_prng_fill_device(modlin_prng* g, uint64_t p, uint64_t* d_out, size_t count, void* stream) {
+  if (!g || (!d_out && count)) return MODLIN_EINVAL_ARG;
+  FieldParams fp{};
+  if (p && !make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!count) return MODLIN_OK;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g_(C->mu);
+  uint64_t nl = 0;
+  rc = prng_fill_device(C->prng, C->num_sms, g, p, fp, d_out, count, user_stream(stream), &nl);
+  g_launches += nl;
+  return rc;
+}
+
+int modlin_rank_prng(uint64_t p, modlin_prng* g, size_t n, const modlin_rank_opts* opts, size_t* rank_out,
+                     modlin_progress_fn cb, void* cb_ctx) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (n == 0 || n > 0x7fffffff / 2 || n > SIZE_MAX / n / 8) return MODLIN_EINVAL_N;
+  if (!g || !rank_out) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g_(C->mu);
+  CK(C->mat.ensure(n * n * 8));
+  uint64_t nl = 0;
+  rc = prng_fill_device(C->prng, C->num_sms, g, p, fp, C->mat.as<uint64_t>(), (uint64_t)n * n, C->stream, &nl);
+  g_launches += nl;
+  if (rc) return rc;
+  return rank_device_locked(C, p, C->mat.as<uint64_t>(), n, opts, rank_out, nullptr, C->stream, cb, cb_ctx);
 }
 
 uint64_t modlin_kernel_launches(void) { return g_launches.load(); }

@@ -245,19 +245,18 @@ int main(int argc, char** argv) {
     std::printf("Running a modular rank test using %s of RAM: %" PRIu64 " %zu×%zu %s over the field of size %" PRIu64 "\n",
                 format_memory((double)n * n * 8).c_str(), reps, n, n, reps == 1 ? "matrix" : "matrices", modulus);
     std::fflush(stdout);
-    std::vector<uint64_t> data(n * n);
+    // Each matrix is the next n*n outputs reduced mod p (src/main.rs:94-104),
+    // generated in device memory and ranked there.
     for (uint64_t i = 0; i < reps; ++i) {
-      modlin_prng_fill(rng, data.data(), data.size());
-      for (auto& x : data) x = modlin_field_reduce(&field, x);
       const auto t0 = std::chrono::steady_clock::now();
       size_t r = 0;
-      const int rc = modlin_rank_ex(modulus, data.data(), n, &ropts, &r, nullptr, progress_cb, &pr);
+      const int rc = modlin_rank_prng(modulus, rng, n, &ropts, &r, progress_cb, &pr);
       if (rc) {
         std::fprintf(stderr, "rank failed: %s\n", modlin_strerror(rc));
         return 1;
       }
       const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      std::fprintf(stderr, "Matrix %" PRIu64 "/%" PRIu64 ": ranked in %.3f ms\n", i + 1, reps, ms);
+      std::fprintf(stderr, "Matrix %" PRIu64 "/%" PRIu64 ": generated and ranked in %.3f ms\n", i + 1, reps, ms);
       const size_t corank = n - r;
       std::printf("Matrix %" PRIu64 "/%" PRIu64 "\tcorank=%zu\tp=%s\n", i + 1, reps, corank,
                   pretty(modlin_corank_tail_pvalue(modulus, n, corank)).c_str());

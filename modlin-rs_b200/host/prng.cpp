@@ -1,130 +1,14 @@
-// Generators under test (host): xoroshiro128++ and MIXMAX over 2^61 - 1.
-//
-// Restates src/prng.rs of the modlin crate, which selects one generator per
-// build through a Cargo feature; here the kind is a runtime argument so one
-// library serves every -R/-L run. MIXMAX is ROOT's MixMaxEngine<N, skip>
-// (seed_spbox seeding, iterate_raw_vec, 61-bit outputs shifted left by 3).
+// Generators under test, host side: construction, names and the sequential
+// stream (src/prng.rs). The state and step live in prng.h.
 #include <cstdint>
 #include <cstring>
 #include <new>
 
 #include "../../include/modlin.h"
+#include "prng.h"
 
-namespace {
-
-constexpr uint64_t kMP = 2305843009213693951ULL;  // 2^61 - 1
-constexpr int kMBits = 61;
-
-inline uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
-inline uint64_t mersenne_fold(uint64_t k) { return (k & kMP) + (k >> kMBits); }  // non-canonical, as ROOT
-
-struct Xoroshiro {
-  uint64_t s0, s1;
-  explicit Xoroshiro(uint64_t seed) {  // src/prng.rs:58-72: SplitMix64 expansion
-    uint64_t z = seed;
-    auto sm = [&z]() {
-      z += 0x9e3779b97f4a7c15ULL;
-      uint64_t w = z;
-      w = (w ^ (w >> 30)) * 0xbf58476d1ce4e5b9ULL;
-      w = (w ^ (w >> 27)) * 0x94d049bb133111ebULL;
-      return w ^ (w >> 31);
-    };
-    s0 = sm();
-    s1 = sm();
-  }
-  uint64_t next() {  // src/prng.rs:75-83
-    const uint64_t a = s0;
-    uint64_t b = s1;
-    const uint64_t r = rotl(a + b, 17) + a;
-    b ^= a;
-    s0 = rotl(a, 49) ^ b ^ (b << 21);
-    s1 = rotl(b, 28);
-    return r;
-  }
-};
-
-// MixMax<N, SPECIALMUL, SPECIAL, SKIP> (src/prng.rs:133-270).
-struct MixMax {
-  int N, specialmul, skip;
-  uint64_t special;  // UINT64_MAX stands for ROOT's -1 (N = 256)
-  uint64_t v[256];
-  uint64_t sumtot;
-  int counter;
-
-  static uint64_t fmodmul(uint64_t cum, uint64_t a, uint64_t b) {  // src/prng.rs:117-127
-    const unsigned __int128 s = (unsigned __int128)a * b + cum;
-    const uint64_t lo = (uint64_t)s, hi = (uint64_t)(s >> 64);
-    return mersenne_fold((lo & kMP) + hi * 8 + (lo >> kMBits));
-  }
-
-  bool seed(uint64_t sd) {  // src/prng.rs:152-176, ROOT seed_spbox
-    if (sd == 0) return false;
-    uint64_t l = sd, acc = 0, ovf = 0;
-    for (int i = 0; i < N; ++i) {
-      l *= 6364136223846793005ULL;
-      l = (l << 32) ^ (l >> 32);
-      v[i] = l & kMP;
-      const uint64_t t = acc + v[i];
-      ovf += t < acc;
-      acc = t;
-    }
-    sumtot = mersenne_fold(mersenne_fold(acc) + (ovf << 3));
-    counter = N;
-    return true;
-  }
-
-  void iterate() {  // src/prng.rs:191-222
-    const uint64_t temp2 = v[1];
-    uint64_t tv = sumtot, acc = tv, ovf = 0, tp = 0;
-    v[0] = tv;
-    for (int i = 1; i < N; ++i) {
-      if (specialmul) {
-        const uint64_t tpo = ((tp << specialmul) & kMP) | (tp >> (kMBits - specialmul));
-        tp = mersenne_fold(tp + v[i]);
-        tv = mersenne_fold(tv + tp + tpo);
-      } else {
-        tp = mersenne_fold(tp + v[i]);
-        tv = mersenne_fold(tv + tp);
-      }
-      v[i] = tv;
-      const uint64_t t = acc + tv;
-      ovf += t < acc;
-      acc = t;
-    }
-    if (special) {
-      const uint64_t t2 = special == UINT64_MAX ? kMP - temp2 : fmodmul(0, special, temp2);
-      v[2] = mersenne_fold(v[2] + t2);
-      const uint64_t t = acc + t2;
-      ovf += t < acc;
-      acc = t;
-    }
-    sumtot = mersenne_fold(mersenne_fold(acc) + (ovf << 3));
-  }
-
-  uint64_t next() {  // src/prng.rs:243-269: next_raw() << 3
-    const int c = counter;
-    if (c >= N)
-      for (int k = 0; k < skip; ++k) iterate();
-    counter = c;
-    uint64_t raw;
-    if (counter < N) {
-      raw = v[counter++];
-    } else {
-      iterate();
-      counter = 2;
-      raw = v[1];
-    }
-    return raw << 3;
-  }
-};
-
-}  // namespace
-
-struct modlin_prng {
-  int kind;
-  Xoroshiro* xo;
-  MixMax* mm;
-};
+using modlin_prng_impl::MixMax;
+using modlin_prng_impl::Xoroshiro;
 
 extern "C" modlin_prng* modlin_prng_new(int kind, uint64_t seed, int* err) {
   auto* g = new (std::nothrow) modlin_prng{kind, nullptr, nullptr};
@@ -176,4 +60,45 @@ extern "C" void modlin_prng_free(modlin_prng* g) {
   delete g->xo;
   delete g->mm;
   delete g;
+}
+
+extern "C" size_t modlin_prng_state_words(int kind) {
+  switch (kind) {
+    case MODLIN_PRNG_XOROSHIRO128PP: return 2;
+    case MODLIN_PRNG_MIXMAX17: return 17 + 2;
+    case MODLIN_PRNG_MIXMAX240: return 240 + 2;
+    case MODLIN_PRNG_MIXMAX256: return 256 + 2;
+    default: return 0;
+  }
+}
+
+extern "C" int modlin_prng_get_state(const modlin_prng* g, uint64_t* words, size_t n) {
+  if (!g || !words || n != modlin_prng_state_words(g->kind)) return MODLIN_EINVAL_ARG;
+  if (g->xo) {
+    words[0] = g->xo->s0;
+    words[1] = g->xo->s1;
+  } else {
+    const MixMax& m = *g->mm;
+    for (int i = 0; i < m.N; ++i) words[i] = m.v[i];
+    words[m.N] = m.sumtot;
+    words[m.N + 1] = (uint64_t)m.counter;
+  }
+  return MODLIN_OK;
+}
+
+extern "C" int modlin_prng_set_state(modlin_prng* g, const uint64_t* words, size_t n) {
+  if (!g || !words || n != modlin_prng_state_words(g->kind)) return MODLIN_EINVAL_ARG;
+  if (g->xo) {
+    g->xo->s0 = words[0];
+    g->xo->s1 = words[1];
+    return MODLIN_OK;
+  }
+  MixMax& m = *g->mm;
+  for (int i = 0; i <= m.N; ++i)
+    if (words[i] > modlin_prng_impl::kMP) return MODLIN_EINVAL_ARG;
+  if (words[m.N + 1] < 1 || words[m.N + 1] > (uint64_t)m.N) return MODLIN_EINVAL_ARG;
+  for (int i = 0; i < m.N; ++i) m.v[i] = words[i];
+  m.sumtot = words[m.N];
+  m.counter = (int)words[m.N + 1];
+  return MODLIN_OK;
 }

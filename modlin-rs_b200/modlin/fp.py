@@ -88,6 +88,17 @@ def rank_device(field, ptr: int, n: int, *, kernel: str = "auto", stream: int = 
     return (r, [int(x) for x in pc[:r]]) if pivot_cols else r
 
 
+def rank_prng(field, gen, n: int, *, kernel: str = "auto", progress=None) -> int:
+    """Rank of the next n x n outputs of ``gen`` (a ``prng.Prng``) reduced
+    mod p, generated and ranked in device memory (src/main.rs:94-112)."""
+    opts = RankOpts(KERNELS[kernel], 0)
+    out = szt(0)
+    cb = PROGRESS(lambda ctx, done, total: progress(done, total)) if progress else _NO_PROGRESS
+    check(lib().modlin_rank_prng(_p(field), gen.handle, n, ctypes.byref(opts), ctypes.byref(out), cb, None),
+          "rank_prng")
+    return int(out.value)
+
+
 def linear_complexity(field, s, *, kernel: str = "auto", grid_ctas: int = 0, check_input: bool = False) -> int:
     """``fp::linear_complexity`` (src/fp.rs:260)."""
     a = _as_u64(s)

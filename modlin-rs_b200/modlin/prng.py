@@ -32,6 +32,25 @@ class Prng:
     def next_u64(self) -> int:
         return int(self.fill(1)[0])
 
+    def fill_device(self, ptr: int, count: int, p: int = 0, stream: int = 0) -> None:
+        """The next ``count`` outputs written to device memory at ``ptr``
+        (reduced mod ``p`` unless 0); bit-identical to ``fill``."""
+        check(lib().modlin_prng_fill_device(self._g, p, ptr, count, stream or None), "prng_fill_device")
+
+    def get_state(self) -> np.ndarray:
+        n = lib().modlin_prng_state_words(self._k)
+        out = np.zeros(n, dtype=np.uint64)
+        check(lib().modlin_prng_get_state(self._g, out.ctypes.data_as(u64p), n), "prng_get_state")
+        return out
+
+    def set_state(self, words) -> None:
+        a = np.ascontiguousarray(np.asarray(words, dtype=np.uint64))
+        check(lib().modlin_prng_set_state(self._g, a.ctypes.data_as(u64p), a.size), "prng_set_state")
+
+    @property
+    def handle(self):
+        return self._g
+
     def __del__(self):
         g = getattr(self, "_g", None)
         if g:

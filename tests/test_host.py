@@ -171,3 +171,59 @@ def test_cli_seed_parsing(built_lib):
         assert lines[:2] == ["Generator: xoroshiro128++", "Seed: 0x%016x" % v], r.stdout
         assert lines[2] == ("Running a modular rank test using 0.000 MiB of RAM: 1 2\u00d72 matrix "
                             "over the field of size 7")
+
+
+def test_prng_state_roundtrip(M):
+    """modlin_prng_get_state / set_state: a saved position replays the stream."""
+    for kind, words in [("xoroshiro128pp", 2), ("mixmax17", 19), ("mixmax", 242), ("mixmax256", 258)]:
+        g = M.prng.Prng(kind, 9)
+        g.fill(1234)
+        s = g.get_state()
+        assert s.size == words
+        a = g.fill(777)
+        g.set_state(s)
+        assert np.array_equal(g.fill(777), a)
+    g = M.prng.Prng("mixmax17", 9)
+    s = g.get_state()
+    for i, bad in [(3, 1 << 61), (17, 1 << 62), (18, 0), (18, 18)]:
+        t = s.copy()
+        t[i] = bad
+        with pytest.raises(M.ModlinError):
+            g.set_state(t)
+    with pytest.raises(M.ModlinError):
+        g.set_state(s[:-1])
+
+
+@pytest.mark.parametrize("kind", ["mixmax17", "mixmax", "mixmax256"])
+def test_mixmax_is_linear_over_fp(M, kind):
+    """The device fill's jump-ahead rests on this: block b of the stream is
+    (skip + 1) linear iterations of block b - 1 over F_p (outputs >> 3 are
+    the raw state entries v[1..N-1])."""
+    from mixmax_model import MIX, mix_step
+    N, _, skip, _ = MIX[kind]
+    g = M.prng.Prng(kind, 5)
+    st = g.get_state()
+    y = [int(st[N])] + [int(v) for v in st[1:N]]
+    out = g.fill(6 * (N - 1))
+    for b in range(6):
+        for _ in range(skip + 1):
+            y = mix_step(kind, y)
+        got = [(int(v) >> 3) % M61 for v in out[b * (N - 1):(b + 1) * (N - 1)]]
+        assert got == y[1:], (kind, b)
+
+
+@pytest.mark.parametrize("kind", ["mixmax17", "mixmax256"])
+def test_mixmax_folds_keep_p_for_zero(M, kind):
+    """ROOT's single fold leaves 2^61 - 1 (not 0) where a sum of nonzero
+    residues is = 0, and that reaches the output as (2^61 - 1) << 3: states
+    planted to hit such sums produce it, so a fill that computes canonical
+    residues alone would differ there."""
+    from mixmax_model import MIX, plant, set_mix_state
+    N, _, skip, _ = MIX[kind]
+    per = skip + 1
+    x = plant(kind, np.random.default_rng(1), [(per, 5), (2 * per, N - 1)])
+    g = M.prng.Prng(kind, 1)
+    set_mix_state(g, kind, x, N)
+    out = g.fill(2 * (N - 1))
+    p3 = np.uint64((M61 << 3) & ((1 << 64) - 1))
+    assert out[4] == p3 and out[N - 1 + N - 2] == p3
