@@ -529,6 +529,52 @@ def rank_planted_measure(torch, modlin, n=16384, L=4096, seed=8, steps=1):
     return res
 
 
+def prng_fill_measure(torch, modlin, count=1 << 32, host_sample=1 << 23, readme_side=65536):
+    """The generators' device fill (modlin_prng_fill_device) of the README's
+    largest job, 2^32 outputs reduced mod 2^61-1 (a 65536^2 matrix), for
+    MIXMAX-256 and xoroshiro128++, against the host stream's rate; then that
+    whole job (generate + rank, modlin_rank_prng): MIXMAX-256 seed 1 has
+    corank 65536 - 65280 = 256 (README.md:98-113)."""
+    from modlin import fp as mfp
+    out = torch.empty(count, dtype=torch.int64, device="cuda")
+    peak = measured_peaks().get("hbm_gbs", 6650.0)
+    res = {"outputs": count}
+    for kind in ("mixmax256", "xoroshiro128pp"):
+        g = modlin.prng.Prng(kind, 1)
+        g.fill_device(out.data_ptr(), 1 << 20, M61)  # warm-up: jump matrices, workspace
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        g.fill_device(out.data_ptr(), count, M61)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1)
+        h = modlin.prng.Prng(kind, 1)
+        h.fill(1 << 20)
+        t0 = time.perf_counter()
+        h.fill(host_sample)
+        hs = time.perf_counter() - t0
+        gbs = 8 * count / (ms * 1e-3) / 1e9
+        res[kind] = {"ms": ms, "wall_ms": wall * 1e3, "outputs_per_s": count / (ms * 1e-3), "write_gbs": gbs,
+                     "hbm_frac_of_measured": gbs / peak,
+                     "host_outputs_per_s": host_sample / hs,
+                     "speedup_vs_host_fill": (count / (ms * 1e-3)) / (host_sample / hs)}
+    del out
+    torch.cuda.empty_cache()
+    g = modlin.prng.Prng("mixmax256", 1)
+    t0 = time.perf_counter()
+    r = mfp.rank_prng(M61, g, readme_side)
+    job_s = time.perf_counter() - t0
+    assert readme_side - r == 256, r
+    res["readme_rank_job"] = {"side": readme_side, "generator": "MIXMAX-256 seed 1", "corank": readme_side - r,
+                              "seconds": job_s,
+                              "note": "README.md:110-113: 'a couple of hours' for the reference on a CPU"}
+    torch.cuda.empty_cache()
+    return res
+
+
 def host_cores():
     try:
         import oracle
@@ -706,6 +752,8 @@ def main():
         extras["rank_planted"] = rank_planted_measure(torch, modlin)
         # Batched rank: 4096 matrices of sides 64..1024 in one launch.
         extras["rank_batch"] = rank_batch_measure(torch, modlin, steps=1, warmup=1, single_sample=16)
+        # The generators' device fill and the README's largest rank job.
+        extras["prng_fill"] = prng_fill_measure(torch, modlin)
 
     # End to end through the public C ABI with host buffers: pinned host
     # matrix -> modlin_rank (H2D copy + rank + D2H of the result) each step.
