@@ -112,6 +112,13 @@ int modlin_rank_prng(uint64_t p, modlin_prng *g, size_t n, const modlin_rank_opt
 int modlin_trailing_update_device(uint64_t p, uint64_t *d_C, size_t ldc, size_t M, size_t N,
                                   const uint64_t *d_L, const uint64_t *d_U, size_t ldu, size_t K,
                                   int kernel, void *stream);
+/* The multiplier block of one block step of the rank (the pivot block's
+ * inverse; the reference's in-panel elimination, src/fp.rs:146-200, as one
+ * device operation): P is 64 x 64 at d_P (row stride ldp >= 64), entries in
+ * [0, p); d_out (64 x 64, row stride 64) receives -P^-1, row c belonging to
+ * column c of P; *singular = 1 (d_out unspecified) when P is singular. */
+int modlin_block_inverse_device(uint64_t p, const uint64_t *d_P, size_t ldp, uint64_t *d_out, int *singular,
+                                void *stream);
 
 /* ---- Linear complexity (src/fp.rs:257-308) ------------------------------ */
 

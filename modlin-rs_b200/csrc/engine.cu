@@ -93,6 +93,7 @@ struct Ctx {
   DevBuf batchm, rbjobs, rbout;  // batched rank: matrix arena, jobs, ranks
   DevBuf tunebuf;                // autotuner inputs
   PrngCache prng;                // generator fills: jump matrices, workspace
+  DevBuf invst;                  // status word of modlin_block_inverse_device
   int64_t* h_out = nullptr;
   std::vector<cudaEvent_t> ev;
 };
@@ -1470,6 +1471,30 @@ int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) 
   CK(reduce_device(fp, d_x, count, st));
   g_launches++;
   return cuda_rc(cudaStreamSynchronize(st));
+}
+
+int modlin_block_inverse_device(uint64_t p, const uint64_t* d_P, size_t ldp, uint64_t* d_out, int* singular,
+                                 void* stream) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!d_P || !d_out || !singular || ldp < (size_t)kPanel) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g_(C->mu);
+  cudaStream_t st = user_stream(stream);
+  CK(C->invst.ensure(sizeof(int)));
+  CK(cudaMemsetAsync(C->invst.p, 0, sizeof(int), st));
+  if (p == kM61)
+    launch_block_inverse<FpM61>(FpM61(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st);
+  else
+    launch_block_inverse<FpBarrett>(FpBarrett(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st);
+  g_launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(C->h_out, C->invst.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *singular = (int)*reinterpret_cast<int*>(C->h_out);
+  return MODLIN_OK;
 }
 
 int modlin_prng_fill_device(modlin_prng* g, uint64_t p, uint64_t* d_out, size_t count, void* stream) {

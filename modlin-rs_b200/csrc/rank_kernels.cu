@@ -327,9 +327,9 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
 }
 
 // ---------------------------------------------------------------------------
-// block_inverse_kernel — one CTA of 1024 threads (16 per block row): the
-// inverse of the 64 x 64 block P = A[r0 .. r0+64, col .. col+64), or
-// status = 1 when P is singular. In-place fraction-free Gauss-Jordan: at
+// gj64_inverse — one CTA of 1024 threads (16 per block row): the inverse of
+// the 64 x 64 block P = A[r0 .. r0+64, col .. col+64), or status = 1 when P
+// is singular. In-place fraction-free Gauss-Jordan: at
 // column c with pivot row `piv` (the first row not yet used whose entry is
 // nonzero) every other row j becomes e * row_j - h * row_piv (e = P[piv][c],
 // h = P[j][c]: one reduction of the two-product sum per entry), and column c,
@@ -344,10 +344,8 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
 // block row), the B operand of the multiplier GEMM H = X_P * P^-1.
 // ---------------------------------------------------------------------------
 template <class F>
-__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
-                                                                     int32_t r0, int32_t col,
-                                                                     uint64_t* __restrict__ Vneg, int* status) {
-  extern __shared__ __align__(16) uint64_t smem_inv[];
+__device__ void gj64_inverse(const F& f, const uint64_t* __restrict__ m, int64_t ld, int32_t r0, int32_t col,
+                             uint64_t* __restrict__ Vneg, int* status, uint64_t* smem_inv) {
   uint64_t(*M)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv);
   __shared__ uint64_t d[kPanel], dinv[kPanel], sc[kPanel];
   __shared__ int32_t pc[kPanel];
@@ -421,6 +419,217 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
     const uint64_t v = f.mul(M[j][pc[i]], dinv[j]);
     Vneg[(int64_t)pc[j] * kPanel + i] = v ? p - v : 0;
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// Recursive fraction-free inverse of the 64 x 64 block (the fast path of
+// block_inverse_kernel). With P = [[A, B], [C, D]] in h x h blocks and
+// A^-1 = N1 / d1 (numerator, scalar denominator):
+//   S' = d1 D - (C N1) B  (= d1 S, S the Schur complement), S'^-1 = N2 / d2,
+//   W' = (N1 B) N2, V = N2 (C N1),
+//   P^-1 = [[d2 N1 + W' (C N1), -d1 W'], [-d1 V, d1^2 N2]] / (d1 d2).
+// Blocks of 32 recurse the same way; blocks of 16 are fraction-free
+// Gauss-Jordan on [X | I] with first-nonzero pivoting inside the block (256
+// threads, two entries each, one named barrier per column), after which row
+// j reads [D_j at its pivot column | D_j X^-1 row], and the per-row D_j are
+// brought to their product. No modular inverse until the single one of the
+// final denominator. The leading 16- and 32-blocks and their Schur
+// complements must be invertible; when one is not, the caller falls back to
+// gj64_inverse (pivoting over all 64 rows), so the result never depends on
+// that. Every product sum is exact (lazy u128 accumulation, one reduction
+// per safe_batch products).
+// ---------------------------------------------------------------------------
+constexpr int kRecWords = 64 * 64 * 2 + 7 * 32 * 32 + 7 * 16 * 16 + 16 * 16;  // X, Out, scratch, base's I
+
+struct RecShared {
+  uint64_t pe[16];
+  int32_t pc[16];
+  uint8_t nz[2][16];
+  int fail;
+};
+
+__device__ __forceinline__ void bar_base() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+template <class F, int K>
+__device__ __forceinline__ uint64_t rec_dot(const F& f, const uint64_t* A, const uint64_t* B, int ldb) {
+  const uint64_t sb = f.safe_batch();
+  u128 acc = 0;
+  if (sb >= (uint64_t)K) {
+#pragma unroll 16
+    for (int k = 0; k < K; ++k) acc += f.prod(A[k], B[k * ldb]);
+  } else {
+    uint64_t cnt = 0;
+    for (int k = 0; k < K; ++k) {
+      acc += f.prod(A[k], B[k * ldb]);
+      if (++cnt == sb) {
+        acc = f.reduce(acc);
+        cnt = 1;
+      }
+    }
+  }
+  return f.reduce(acc);
+}
+
+// 16 x 16 block X (clobbered) -> Out = X^-1 * delta, delta = product of the
+// rows' final pivot entries. All threads call; threads 0..255 work.
+template <class F>
+__device__ void rec_base16(const F& f, uint64_t* X, int ldx, uint64_t* R, uint64_t* Out, int ldo, uint64_t* delta,
+                           RecShared& S) {
+  const uint64_t p = f.modulus();
+  const int tid = threadIdx.x;
+  if (tid < 256) {
+    const int j = tid >> 4, k = tid & 15, lane = tid & 31;
+    uint64_t x = X[j * ldx + k], y = j == k;
+    R[j * 16 + k] = y;
+    if (k == 0) S.nz[0][j] = x != 0;
+    bar_base();
+    unsigned used = 0;
+    bool ok = true;
+    for (int c = 0; c < 16; ++c) {
+      const unsigned b = __ballot_sync(0xffffffffu, lane < 16 && !((used >> lane) & 1) && S.nz[c & 1][lane & 15]);
+      if (b == 0) {
+        ok = false;
+        break;
+      }
+      const int piv = __ffs(b) - 1;
+      const uint64_t e = X[piv * ldx + c], h = X[j * ldx + c];
+      const uint64_t xp = X[piv * ldx + k], yp = R[piv * 16 + k];
+      __syncwarp();  // row j's reads of X[j][c] precede its owner's write below
+      if (j != piv && h != 0) {
+        const uint64_t nh = p - h;
+        x = f.reduce2(f.prod(e, x) + f.prod(nh, xp));
+        y = f.reduce2(f.prod(e, y) + f.prod(nh, yp));
+        X[j * ldx + k] = x;
+        R[j * 16 + k] = y;
+      }
+      if (j == piv && k == 0) S.pc[j] = c;
+      if (k == c + 1) S.nz[(c + 1) & 1][j] = x != 0;
+      used |= 1u << piv;
+      bar_base();
+    }
+    if (!ok) {
+      if (tid == 0) S.fail = 1;
+    } else {
+      if (tid < 32) {  // pe[j] = product of the other rows' pivot entries
+        const uint64_t xd = lane < 16 ? X[lane * ldx + S.pc[lane]] : 1;
+        uint64_t pre = xd, suf = xd;
+#pragma unroll
+        for (int off = 1; off < 16; off <<= 1) {
+          const uint64_t a = __shfl_up_sync(0xffffffffu, pre, off), b2 = __shfl_down_sync(0xffffffffu, suf, off);
+          if (lane >= off) pre = f.mul(pre, a);
+          if (lane + off < 16) suf = f.mul(suf, b2);
+        }
+        const uint64_t ex_pre = __shfl_up_sync(0xffffffffu, pre, 1), ex_suf = __shfl_down_sync(0xffffffffu, suf, 1);
+        const uint64_t all = __shfl_sync(0xffffffffu, pre, 15);
+        if (lane < 16) S.pe[lane] = f.mul(lane ? ex_pre : 1, lane < 15 ? ex_suf : 1);
+        if (lane == 0) *delta = all;
+      }
+      bar_base();
+      Out[S.pc[j] * ldo + k] = f.mul(y, S.pe[j]);
+    }
+  }
+  __syncthreads();
+}
+
+// N x N block X (N = 32 or 64; its top-left h x h block is clobbered) ->
+// Out = X^-1 * delta. Scratch: 7 h x h buffers at scr, then the next level's.
+template <class F, int N>
+__device__ void rec_inverse(const F& f, uint64_t* X, int ldx, uint64_t* Out, int ldo, uint64_t* delta, uint64_t* scr,
+                            uint64_t* R, RecShared& S, uint64_t* dl) {
+  constexpr int H = N / 2, HH = H * H;
+  const uint64_t p = f.modulus();
+  uint64_t *N1 = scr, *CN = scr + HH, *NB = scr + 2 * HH, *Sp = scr + 3 * HH, *N2 = scr + 4 * HH, *Wp = scr + 5 * HH,
+           *V = scr + 6 * HH;
+  uint64_t* A = X;
+  const uint64_t *B = X + H, *C = X + H * ldx, *D = X + H * ldx + H;
+  if constexpr (H == 16)
+    rec_base16(f, A, ldx, R, N1, H, &dl[0], S);
+  else
+    rec_inverse<F, H>(f, A, ldx, N1, H, &dl[0], scr + 7 * HH, R, S, dl + 2);
+  if (S.fail) return;
+  const uint64_t d1 = dl[0];
+  for (int t = threadIdx.x; t < 2 * HH; t += blockDim.x) {  // CN = C N1, NB = N1 B
+    const int u = t & (HH - 1), i = u / H, j = u % H;
+    if (t < HH)
+      CN[u] = rec_dot<F, H>(f, C + i * ldx, N1 + j, H);
+    else
+      NB[u] = rec_dot<F, H>(f, N1 + i * H, B + j, ldx);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < HH; t += blockDim.x) {  // S' = d1 D - CN B
+    const int i = t / H, j = t % H;
+    const uint64_t v = rec_dot<F, H>(f, CN + i * H, B + j, ldx);
+    Sp[t] = f.sub(f.mul(d1, D[i * ldx + j]), v);
+  }
+  __syncthreads();
+  if constexpr (H == 16)
+    rec_base16(f, Sp, H, R, N2, H, &dl[1], S);
+  else
+    rec_inverse<F, H>(f, Sp, H, N2, H, &dl[1], scr + 7 * HH, R, S, dl + 2);
+  if (S.fail) return;
+  const uint64_t d2 = dl[1];
+  for (int t = threadIdx.x; t < 2 * HH; t += blockDim.x) {  // W' = NB N2, V = N2 CN
+    const int u = t & (HH - 1), i = u / H, j = u % H;
+    if (t < HH)
+      Wp[u] = rec_dot<F, H>(f, NB + i * H, N2 + j, H);
+    else
+      V[u] = rec_dot<F, H>(f, N2 + i * H, CN + j, H);
+  }
+  __syncthreads();
+  const uint64_t d11 = f.mul(d1, d1);
+  for (int t = threadIdx.x; t < 4 * HH; t += blockDim.x) {  // [[d2 N1 + W' CN, -d1 W'], [-d1 V, d1^2 N2]]
+    const int q = t / HH, u = t & (HH - 1), i = u / H, j = u % H;
+    uint64_t v;
+    if (q == 0) {
+      v = f.add(f.mul(d2, N1[u]), rec_dot<F, H>(f, Wp + i * H, CN + j, H));
+    } else if (q == 3) {
+      v = f.mul(d11, N2[u]);
+    } else {
+      v = f.mul(d1, q == 1 ? Wp[u] : V[u]);
+      v = v ? p - v : 0;
+    }
+    Out[(i + (q >> 1) * H) * ldo + j + (q & 1) * H] = v;
+  }
+  if (threadIdx.x == 0) *delta = f.mul(d1, d2);
+  __syncthreads();
+}
+
+// block_inverse_kernel: the recursive path when `rec` (large p: a singular
+// leading sub-block has probability about 4/p), else or on its failure the
+// pivoting Gauss-Jordan. Output as gj64_inverse.
+template <class F>
+__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
+                                                                     int32_t r0, int32_t col,
+                                                                     uint64_t* __restrict__ Vneg, int* status, int rec) {
+  extern __shared__ __align__(16) uint64_t smem_inv[];
+  if (rec) {
+    __shared__ RecShared S;
+    __shared__ uint64_t dl[5];  // level 64: d1, d2; level 32: d1, d2; the result's denominator
+    __shared__ uint64_t invd;
+    uint64_t* X = smem_inv;
+    uint64_t* Out = X + 64 * 64;
+    uint64_t* scr = Out + 64 * 64;
+    uint64_t* R = scr + 7 * 32 * 32 + 7 * 16 * 16;
+    for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x)
+      X[t] = m[(int64_t)(r0 + (t >> 6)) * ld + col + (t & 63)];
+    if (threadIdx.x == 0) S.fail = 0;
+    __syncthreads();
+    rec_inverse<F, 64>(f, X, 64, Out, 64, &dl[4], scr, R, S, dl);
+    if (!S.fail) {
+      const uint64_t p = f.modulus();
+      if (threadIdx.x == 0) invd = fp_inv_binary(dl[4], p);
+      __syncthreads();
+      const uint64_t inv = invd;
+      for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) {
+        const uint64_t v = f.mul(Out[t], inv);
+        Vneg[t] = v ? p - v : 0;
+      }
+      return;
+    }
+    __syncthreads();
+  }
+  gj64_inverse(f, m, ld, r0, col, Vneg, status, smem_inv);
 }
 
 // ---------------------------------------------------------------------------
@@ -534,13 +743,14 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int re
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
                           cudaStream_t st) {
-  const size_t smem = kPanel * (kPanel + 1) * sizeof(uint64_t);
+  const size_t smem = kRecWords * sizeof(uint64_t);  // >= the pivoting path's kPanel * (kPanel + 1) words
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(block_inverse_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_set = true;
   }
-  block_inverse_kernel<F><<<1, kInvThreads, smem, st>>>(f, m, ld, r0, col, Vneg, status);
+  const int rec = f.modulus() > (1ULL << 20);
+  block_inverse_kernel<F><<<1, kInvThreads, smem, st>>>(f, m, ld, r0, col, Vneg, status, rec);
 }
 
 template <class F>

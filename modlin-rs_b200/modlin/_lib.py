@@ -93,6 +93,7 @@ def lib():
     _proto(L, "modlin_prng_state_words", szt, [ci])
     _proto(L, "modlin_prng_get_state", ci, [vp, u64p, szt])
     _proto(L, "modlin_prng_set_state", ci, [vp, u64p, szt])
+    _proto(L, "modlin_block_inverse_device", ci, [u64, vp, szt, vp, ctypes.POINTER(ci), vp])
     _proto(L, "modlin_rank_prng", ci, [u64, vp, szt, ctypes.POINTER(RankOpts), sztp, PROGRESS, vp])
     _proto(L, "modlin_gen_uniform", ci, [u64, u64, u64p, szt])
     _proto(L, "modlin_gen_uniform_device", ci, [u64, u64, vp, szt, vp])
@@ -128,6 +129,7 @@ EXPORTED = [
     "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue", "modlin_pretty_p_value",
     "modlin_prng_new", "modlin_prng_name", "modlin_prng_fill", "modlin_prng_free", "modlin_prng_fill_device",
     "modlin_prng_state_words", "modlin_prng_get_state", "modlin_prng_set_state", "modlin_rank_prng",
+    "modlin_block_inverse_device",
     "modlin_gen_uniform", "modlin_gen_uniform_device", "modlin_gen_planted", "modlin_reduce_device",
     "modlin_gen_planted_device", "modlin_gen_planted_batch_device",
     "modlin_kernel_launches", "modlin_last_trailing_ms", "modlin_last_trailing_macs", "modlin_autotune",

@@ -88,6 +88,15 @@ def rank_device(field, ptr: int, n: int, *, kernel: str = "auto", stream: int = 
     return (r, [int(x) for x in pc[:r]]) if pivot_cols else r
 
 
+def block_inverse_device(field, src_ptr: int, ld: int, out_ptr: int, stream: int = 0) -> bool:
+    """-P^-1 of the 64 x 64 block at ``src_ptr`` (row stride ``ld``) into
+    ``out_ptr``; False when P is singular."""
+    sing = ctypes.c_int(0)
+    check(lib().modlin_block_inverse_device(_p(field), src_ptr, ld, out_ptr, ctypes.byref(sing), stream or None),
+          "block_inverse_device")
+    return sing.value == 0
+
+
 def rank_prng(field, gen, n: int, *, kernel: str = "auto", progress=None) -> int:
     """Rank of the next n x n outputs of ``gen`` (a ``prng.Prng``) reduced
     mod p, generated and ranked in device memory (src/main.rs:94-112)."""
