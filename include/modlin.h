@@ -273,8 +273,9 @@ int modlin_reduce_device(uint64_t p, uint64_t *d_x, size_t count, void *stream);
  * MODLIN_LC_AUTO make (no reference counterpart: the reference has one CPU
  * path): the side from which the tensor-core trailing update beats the plain
  * one, per limb count (1, 2, 4 or 8 limbs for p below 2^8, 2^16, 2^32, 2^63;
- * the limb count itself is the smallest exact one); the smallest side for
- * two-panel block steps; Berlekamp-Massey threads per CTA by length, the
+ * the limb count itself is the smallest exact one); the remaining-block size
+ * below which one-panel block steps replace two-panel ones (timed on a
+ * 16384 x 16384 rank); Berlekamp-Massey threads per CTA by length, the
  * block/cluster crossover, and batch threads per CTA by the longest sequence.
  * Takes a few seconds; the choices hold for this process and device. `report`
  * (may be NULL) receives them and the timings as JSON, truncated to cap - 1

@@ -818,34 +818,41 @@ static int autotune_locked(Ctx* C, std::string& rep) {
     T.tc_cross[li] = crossover(sizes, tc_wins, 1 << 30);
   }
   rep += "}";
-  // 2. Two-panel steps against one-panel steps (tensor cores, 2^61 - 1).
+  // 2. The remaining-block size below which one-panel steps replace
+  //    two-panel steps, measured directly on the largest rank (tensor cores,
+  //    2^61 - 1): the late steps' exposed block chain decides it.
   {
-    const std::vector<int> tsz = {256, 512, 1024, 2048, 4096, 8192, 12288, 16384};
-    std::vector<bool> two_wins;
+    const std::vector<int> thr = {0, 2048, 4096, 6144, 8192, 12288, 1 << 30};
     rep += ", \"two_panel_ms\": {";
     const int saved = C->tune.two_panel_min;
-    for (int n : tsz) {
-      uint64_t nl = 0;
-      TK(gen_uniform_device(kM61, 99 + n, pristine, (uint64_t)n * n, st, &nl));
-      float t[2];
-      for (int k = 0; k < 2; ++k) {
-        C->tune.two_panel_min = k == 0 ? (1 << 30) : 0;
-        const modlin_rank_opts o{MODLIN_RANK_TC, 0};
-        size_t r = 0;
-        t[k] = best_ms(C, 2, [&]() -> int {
-          if (cudaMemcpyAsync(work, pristine, (size_t)n * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            return MODLIN_ECUDA;
-          return rank_device_locked(C, kM61, work, n, &o, &r, nullptr, st, nullptr, nullptr);
-        }, &rc);
+    const int n = nmax;
+    uint64_t nl = 0;
+    TK(gen_uniform_device(kM61, 99 + n, pristine, (uint64_t)n * n, st, &nl));
+    float best = 0;
+    int best_thr = saved;
+    for (size_t q = 0; q < thr.size(); ++q) {
+      C->tune.two_panel_min = thr[q];
+      const modlin_rank_opts o{MODLIN_RANK_TC, 0};
+      size_t r = 0;
+      const float t = best_ms(C, 2, [&]() -> int {
+        if (cudaMemcpyAsync(work, pristine, (size_t)n * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+          return MODLIN_ECUDA;
+        return rank_device_locked(C, kM61, work, n, &o, &r, nullptr, st, nullptr, nullptr);
+      }, &rc);
+      if (rc) {
+        C->tune.two_panel_min = saved;
+        return rc;
       }
-      C->tune.two_panel_min = saved;
-      if (rc) return rc;
-      two_wins.push_back(t[1] <= t[0]);
-      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == tsz[0] ? "" : ", ", n, t[0], t[1]);
+      if (q == 0 || t < best) {
+        best = t;
+        best_thr = thr[q];
+      }
+      std::snprintf(buf, sizeof buf, "%s\"below %d\": %.3f", q == 0 ? "" : ", ", thr[q], t);
       rep += buf;
     }
+    C->tune.two_panel_min = saved;
     rep += "}";
-    T.two_panel_min = crossover(tsz, two_wins, 1 << 30);
+    T.two_panel_min = best_thr;
   }
   // 3. Batched rank: tensor-core kernel against the integer-pipe kernel, per
   //    side (a batch of two matrices per SM, 2^61 - 1).

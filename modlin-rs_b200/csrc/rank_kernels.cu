@@ -430,22 +430,21 @@ __device__ void gj64_inverse(const F& f, const uint64_t* __restrict__ m, int64_t
 //   W' = (N1 B) N2, V = N2 (C N1),
 //   P^-1 = [[d2 N1 + W' (C N1), -d1 W'], [-d1 V, d1^2 N2]] / (d1 d2).
 // Blocks of 32 recurse the same way; blocks of 16 are fraction-free
-// Gauss-Jordan on [X | I] with first-nonzero pivoting inside the block (256
-// threads, two entries each, one named barrier per column), after which row
-// j reads [D_j at its pivot column | D_j X^-1 row], and the per-row D_j are
-// brought to their product. No modular inverse until the single one of the
-// final denominator. The leading 16- and 32-blocks and their Schur
-// complements must be invertible; when one is not, the caller falls back to
-// gj64_inverse (pivoting over all 64 rows), so the result never depends on
-// that. Every product sum is exact (lazy u128 accumulation, one reduction
+// Gauss-Jordan on [X | I] with diagonal pivots (256 threads, two entries
+// each, one named barrier per column), after which row j reads
+// [D_j at column j | D_j X^-1 row j], and the per-row D_j are brought to
+// their product. No modular inverse until the single one of the final
+// denominator. The diagonal pivots and the leading 16- and 32-blocks and
+// their Schur complements must be nonzero / invertible (for large p all
+// fail with probability about 100/p); when one is not, the caller falls
+// back to gj64_inverse (first-nonzero pivoting over all 64 rows), so the
+// result never depends on that. Every product sum is exact (lazy u128 accumulation, one reduction
 // per safe_batch products).
 // ---------------------------------------------------------------------------
 constexpr int kRecWords = 64 * 64 * 2 + 7 * 32 * 32 + 7 * 16 * 16 + 16 * 16;  // X, Out, scratch, base's I
 
 struct RecShared {
   uint64_t pe[16];
-  int32_t pc[16];
-  uint8_t nz[2][16];
   int fail;
 };
 
@@ -471,8 +470,19 @@ __device__ __forceinline__ uint64_t rec_dot(const F& f, const uint64_t* A, const
   return f.reduce(acc);
 }
 
+// The dot product of this thread's output with K split over SPLIT adjacent
+// lanes (part = lane's share), summed across them by shuffles.
+template <class F, int K, int SPLIT>
+__device__ __forceinline__ uint64_t rec_dot_split(const F& f, const uint64_t* A, const uint64_t* B, int ldb, int part) {
+  constexpr int KP = K / SPLIT;
+  uint64_t v = rec_dot<F, KP>(f, A + part * KP, B + part * KP * ldb, ldb);
+#pragma unroll
+  for (int o = 1; o < SPLIT; o <<= 1) v = f.add(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // 16 x 16 block X (clobbered) -> Out = X^-1 * delta, delta = product of the
-// rows' final pivot entries. All threads call; threads 0..255 work.
+// rows' final diagonal entries. All threads call; threads 0..255 work.
 template <class F>
 __device__ void rec_base16(const F& f, uint64_t* X, int ldx, uint64_t* R, uint64_t* Out, int ldo, uint64_t* delta,
                            RecShared& S) {
@@ -482,37 +492,31 @@ __device__ void rec_base16(const F& f, uint64_t* X, int ldx, uint64_t* R, uint64
     const int j = tid >> 4, k = tid & 15, lane = tid & 31;
     uint64_t x = X[j * ldx + k], y = j == k;
     R[j * 16 + k] = y;
-    if (k == 0) S.nz[0][j] = x != 0;
     bar_base();
-    unsigned used = 0;
     bool ok = true;
+#pragma unroll 1
     for (int c = 0; c < 16; ++c) {
-      const unsigned b = __ballot_sync(0xffffffffu, lane < 16 && !((used >> lane) & 1) && S.nz[c & 1][lane & 15]);
-      if (b == 0) {
+      const uint64_t e = X[c * ldx + c], h = X[j * ldx + c];
+      if (e == 0) {  // the same in every thread
         ok = false;
         break;
       }
-      const int piv = __ffs(b) - 1;
-      const uint64_t e = X[piv * ldx + c], h = X[j * ldx + c];
-      const uint64_t xp = X[piv * ldx + k], yp = R[piv * 16 + k];
+      const uint64_t xp = X[c * ldx + k], yp = R[c * 16 + k];
       __syncwarp();  // row j's reads of X[j][c] precede its owner's write below
-      if (j != piv && h != 0) {
+      if (j != c && h != 0) {
         const uint64_t nh = p - h;
         x = f.reduce2(f.prod(e, x) + f.prod(nh, xp));
         y = f.reduce2(f.prod(e, y) + f.prod(nh, yp));
         X[j * ldx + k] = x;
         R[j * 16 + k] = y;
       }
-      if (j == piv && k == 0) S.pc[j] = c;
-      if (k == c + 1) S.nz[(c + 1) & 1][j] = x != 0;
-      used |= 1u << piv;
       bar_base();
     }
     if (!ok) {
       if (tid == 0) S.fail = 1;
     } else {
-      if (tid < 32) {  // pe[j] = product of the other rows' pivot entries
-        const uint64_t xd = lane < 16 ? X[lane * ldx + S.pc[lane]] : 1;
+      if (tid < 32) {  // pe[j] = product of the other rows' diagonal entries
+        const uint64_t xd = lane < 16 ? X[lane * ldx + lane] : 1;
         uint64_t pre = xd, suf = xd;
 #pragma unroll
         for (int off = 1; off < 16; off <<= 1) {
@@ -526,7 +530,7 @@ __device__ void rec_base16(const F& f, uint64_t* X, int ldx, uint64_t* R, uint64
         if (lane == 0) *delta = all;
       }
       bar_base();
-      Out[S.pc[j] * ldo + k] = f.mul(y, S.pe[j]);
+      Out[j * ldo + k] = f.mul(y, S.pe[j]);
     }
   }
   __syncthreads();
@@ -548,19 +552,20 @@ __device__ void rec_inverse(const F& f, uint64_t* X, int ldx, uint64_t* Out, int
   else
     rec_inverse<F, H>(f, A, ldx, N1, H, &dl[0], scr + 7 * HH, R, S, dl + 2);
   if (S.fail) return;
+  // Small levels split each dot product over SP lanes (all threads busy).
+  constexpr int SP = H == 16 ? 2 : 1;
   const uint64_t d1 = dl[0];
-  for (int t = threadIdx.x; t < 2 * HH; t += blockDim.x) {  // CN = C N1, NB = N1 B
-    const int u = t & (HH - 1), i = u / H, j = u % H;
-    if (t < HH)
-      CN[u] = rec_dot<F, H>(f, C + i * ldx, N1 + j, H);
-    else
-      NB[u] = rec_dot<F, H>(f, N1 + i * H, B + j, ldx);
+  for (int tt = threadIdx.x; tt < SP * 2 * HH; tt += blockDim.x) {  // CN = C N1, NB = N1 B
+    const int t = tt / SP, part = tt % SP, u = t & (HH - 1), i = u / H, j = u % H;
+    const uint64_t v = t < HH ? rec_dot_split<F, H, SP>(f, C + i * ldx, N1 + j, H, part)
+                              : rec_dot_split<F, H, SP>(f, N1 + i * H, B + j, ldx, part);
+    if (part == 0) (t < HH ? CN : NB)[u] = v;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < HH; t += blockDim.x) {  // S' = d1 D - CN B
-    const int i = t / H, j = t % H;
-    const uint64_t v = rec_dot<F, H>(f, CN + i * H, B + j, ldx);
-    Sp[t] = f.sub(f.mul(d1, D[i * ldx + j]), v);
+  for (int tt = threadIdx.x; tt < SP * HH; tt += blockDim.x) {  // S' = d1 D - CN B
+    const int t = tt / SP, part = tt % SP, i = t / H, j = t % H;
+    const uint64_t v = rec_dot_split<F, H, SP>(f, CN + i * H, B + j, ldx, part);
+    if (part == 0) Sp[t] = f.sub(f.mul(d1, D[i * ldx + j]), v);
   }
   __syncthreads();
   if constexpr (H == 16)
@@ -569,21 +574,23 @@ __device__ void rec_inverse(const F& f, uint64_t* X, int ldx, uint64_t* Out, int
     rec_inverse<F, H>(f, Sp, H, N2, H, &dl[1], scr + 7 * HH, R, S, dl + 2);
   if (S.fail) return;
   const uint64_t d2 = dl[1];
-  for (int t = threadIdx.x; t < 2 * HH; t += blockDim.x) {  // W' = NB N2, V = N2 CN
-    const int u = t & (HH - 1), i = u / H, j = u % H;
-    if (t < HH)
-      Wp[u] = rec_dot<F, H>(f, NB + i * H, N2 + j, H);
-    else
-      V[u] = rec_dot<F, H>(f, N2 + i * H, CN + j, H);
+  for (int tt = threadIdx.x; tt < SP * 2 * HH; tt += blockDim.x) {  // W' = NB N2, V = N2 CN
+    const int t = tt / SP, part = tt % SP, u = t & (HH - 1), i = u / H, j = u % H;
+    const uint64_t v = t < HH ? rec_dot_split<F, H, SP>(f, NB + i * H, N2 + j, H, part)
+                              : rec_dot_split<F, H, SP>(f, N2 + i * H, CN + j, H, part);
+    if (part == 0) (t < HH ? Wp : V)[u] = v;
   }
   __syncthreads();
   const uint64_t d11 = f.mul(d1, d1);
-  for (int t = threadIdx.x; t < 4 * HH; t += blockDim.x) {  // [[d2 N1 + W' CN, -d1 W'], [-d1 V, d1^2 N2]]
+  for (int tt = threadIdx.x; tt < SP * HH; tt += blockDim.x) {  // top left: d2 N1 + W' CN
+    const int t = tt / SP, part = tt % SP, i = t / H, j = t % H;
+    const uint64_t v = rec_dot_split<F, H, SP>(f, Wp + i * H, CN + j, H, part);
+    if (part == 0) Out[i * ldo + j] = f.add(f.mul(d2, N1[t]), v);
+  }
+  for (int t = threadIdx.x + HH; t < 4 * HH; t += blockDim.x) {  // [[., -d1 W'], [-d1 V, d1^2 N2]]
     const int q = t / HH, u = t & (HH - 1), i = u / H, j = u % H;
     uint64_t v;
-    if (q == 0) {
-      v = f.add(f.mul(d2, N1[u]), rec_dot<F, H>(f, Wp + i * H, CN + j, H));
-    } else if (q == 3) {
+    if (q == 3) {
       v = f.mul(d11, N2[u]);
     } else {
       v = f.mul(d1, q == 1 ? Wp[u] : V[u]);
@@ -595,9 +602,9 @@ __device__ void rec_inverse(const F& f, uint64_t* X, int ldx, uint64_t* Out, int
   __syncthreads();
 }
 
-// block_inverse_kernel: the recursive path when `rec` (large p: a singular
-// leading sub-block has probability about 4/p), else or on its failure the
-// pivoting Gauss-Jordan. Output as gj64_inverse.
+// block_inverse_kernel: the recursive path when `rec` (large p, where it
+// fails with probability about 100/p), else or on its failure the pivoting
+// Gauss-Jordan. Output as gj64_inverse.
 template <class F>
 __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
                                                                      int32_t r0, int32_t col,
@@ -633,49 +640,47 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 }
 
 // ---------------------------------------------------------------------------
-// small_gemm64_kernel — one CTA of 1024 threads: C = D - A * B (negate) or
-// C = D + A * B on 64 x 64 blocks mod p (D may be null: zero), operands
-// staged in shared memory, one reduction per output.
+// small_gemm64_kernel — C = D - A * B (negate) or C = D + A * B on 64 x 64
+// blocks mod p (D may be null: zero). 16 CTAs of 256 threads, one 16 x 16
+// output tile each (one output per thread, one reduction per output), so the
+// product spreads over the SMs a finished trailing update leaves free.
 // ---------------------------------------------------------------------------
+constexpr int kSgTile = 16;
 template <class F>
-__global__ void __launch_bounds__(kInvThreads) small_gemm64_kernel(F f, const uint64_t* __restrict__ A, int64_t lda,
-                                                                    const uint64_t* __restrict__ B, int64_t ldb,
-                                                                    const uint64_t* __restrict__ D, int64_t ldd,
-                                                                    uint64_t* __restrict__ Cout, int64_t ldc,
-                                                                    int negate) {
-  extern __shared__ __align__(16) uint64_t smem_g[];
-  uint64_t(*As)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_g);
-  uint64_t(*Bs)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_g + kPanel * (kPanel + 1));
-  const int tid = threadIdx.x, i = tid >> 4, s = tid & 15;
+__global__ void __launch_bounds__(256) small_gemm64_kernel(F f, const uint64_t* __restrict__ A, int64_t lda,
+                                                            const uint64_t* __restrict__ B, int64_t ldb,
+                                                            const uint64_t* __restrict__ D, int64_t ldd,
+                                                            uint64_t* __restrict__ Cout, int64_t ldc, int negate) {
+  __shared__ uint64_t As[kSgTile][kPanel + 1], Bs[kPanel][kSgTile + 1];
+  const int tid = threadIdx.x, i = tid >> 4, j = tid & 15;
+  const int ti = blockIdx.x >> 2, tj = blockIdx.x & 3;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int j = s + 16 * q;
-    As[i][j] = A[(int64_t)i * lda + j];
-    Bs[i][j] = B[(int64_t)i * ldb + j];
+    const int kk = j + 16 * q;
+    As[i][kk] = A[(int64_t)(ti * kSgTile + i) * lda + kk];
+    Bs[i + 16 * q][j] = B[(int64_t)(i + 16 * q) * ldb + tj * kSgTile + j];
   }
   __syncthreads();
   const uint64_t p = f.modulus(), sb = f.safe_batch();
-  // Four independent accumulators (one per output column of this thread).
-  u128 acc[4] = {0, 0, 0, 0};
-  uint64_t cnt = 0;
-  for (int k = 0; k < kPanel; ++k) {
-    const uint64_t a = As[i][k];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] += f.prod(a, Bs[k][s + 16 * q]);
-    if (++cnt == sb) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] = f.reduce(acc[q]);  // counts as one product from here on
-      cnt = 1;
+  u128 acc = 0;
+  if (sb >= (uint64_t)kPanel) {
+#pragma unroll 16
+    for (int k = 0; k < kPanel; ++k) acc += f.prod(As[i][k], Bs[k][j]);
+  } else {
+    uint64_t cnt = 0;
+    for (int k = 0; k < kPanel; ++k) {
+      acc += f.prod(As[i][k], Bs[k][j]);
+      if (++cnt == sb) {
+        acc = f.reduce(acc);  // counts as one product from here on
+        cnt = 1;
+      }
     }
   }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int j = s + 16 * q;
-    uint64_t v = f.reduce(acc[q]);
-    if (negate && v) v = p - v;
-    if (D) v = f.add(v, D[(int64_t)i * ldd + j]);
-    Cout[(int64_t)i * ldc + j] = v;
-  }
+  const int r = ti * kSgTile + i, c = tj * kSgTile + j;
+  uint64_t v = f.reduce(acc);
+  if (negate && v) v = p - v;
+  if (D) v = f.add(v, D[(int64_t)r * ldd + c]);
+  Cout[(int64_t)r * ldc + c] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -756,13 +761,8 @@ void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
                          int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st) {
-  const size_t smem = 2 * kPanel * (kPanel + 1) * sizeof(uint64_t);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(small_gemm64_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
-  }
-  small_gemm64_kernel<F><<<1, kInvThreads, smem, st>>>(f, A, lda, B, ldb, D, ldd, C, ldc, negate ? 1 : 0);
+  small_gemm64_kernel<F><<<(kPanel / kSgTile) * (kPanel / kSgTile), 256, 0, st>>>(f, A, lda, B, ldb, D, ldd, C, ldc,
+                                                                                  negate ? 1 : 0);
 }
 
 #define INSTANTIATE(F)                                                                                          \

@@ -15,6 +15,8 @@ def test_autotune_then_auto_paths_exact(M, O):
     assert ch["bm_threads"] and all(t in (128, 256, 512, 1024) for t in ch["bm_threads"])
     assert all(t in (128, 256, 512) for t in ch["bm_batch_threads"])
     assert ch["bm_cluster_min"] >= 4096
+    assert ch["two_panel_min"] in (0, 2048, 4096, 6144, 8192, 12288, 1 << 30)
+    assert len(rep["two_panel_ms"]) == 7
     assert rep["rank_ms"] and rep["bm_block_ms"] and rep["bm_batch_ms"]
     for p in [127, 65521, 2**31 - 1, M61]:
         for n in [100, 300, 700, 1100]:
