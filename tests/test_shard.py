@@ -86,3 +86,96 @@ def test_run_sharded_gloo_world2(O):
     # Each rank computed a disjoint share, together every job.
     assert sorted(out[0][1] + out[1][1]) == sorted(20 + 7 * i for i in range(12))
     assert out[0][1] and out[1][1]
+
+
+# ---- the column-sharded single rank ------------------------------------------
+
+SHARD_CASES = [("uniform", M61, 200, 0), ("planted", M61, 200, 100), ("uniform", 2, 150, 0),
+               ("uniform", 65521, 130, 0), ("uniform", M61, 40, 0)]
+
+
+def _case_matrix(O, kind, p, n, L):
+    return O.gen_planted(p, L, 9, n * n) if kind == "planted" else O.gen_uniform(p, 9, n * n)
+
+
+def test_sharded_rank_layout():
+    from modlin.shard import local_columns
+    for n in (40, 64, 130, 200, 1000):
+        for world in (1, 2, 3, 5):
+            cols = sorted(c for r in range(world) for c in local_columns(n, r, world))
+            assert cols == list(range(n)), (n, world)
+
+
+def test_sharded_rank_one_process(O):
+    import torch
+    from modlin.shard import rank_sharded, scatter_columns
+    from shard_host_ops import HostOps
+    class Counting(HostOps):
+        steps = 0
+
+        def multipliers(self, *a):
+            Counting.steps += 1
+            return super().multipliers(*a)
+
+    # Block steps taken: every full panel of the uniform matrix over 2^61-1;
+    # one for the planted rank-100 matrix (its second diagonal block lies in
+    # a rank-36 Schur complement, so the rest is gathered there).
+    steps = {("uniform", M61, 200): 3, ("planted", M61, 200): 1, ("uniform", M61, 40): 0}
+    for kind, p, n, L in SHARD_CASES:
+        a = _case_matrix(O, kind, p, n, L)
+        local = torch.from_numpy(scatter_columns(a, n, 0, 1).view(np.int64))
+        Counting.steps = 0
+        assert rank_sharded(p, local, n, ops=Counting(p, O)) == O.rank(p, a, n), (kind, p, n)
+        if (kind, p, n) in steps:
+            assert Counting.steps == steps[(kind, p, n)], (kind, p, n, Counting.steps)
+
+
+def _shard_worker(rank, world, port, q):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    for p in (root, os.path.join(root, "modlin-rs_b200"), here):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    import oracle
+    from modlin.shard import rank_sharded, scatter_columns
+    from shard_host_ops import HostOps
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=120))
+    try:
+        got = []
+        for kind, p, n, L in SHARD_CASES:
+            a = _case_matrix(oracle, kind, p, n, L)
+            local = torch.from_numpy(scatter_columns(a, n, rank, world).view(np.int64))
+            got.append(rank_sharded(p, local, n, ops=HostOps(p, oracle)))
+        q.put((rank, got))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_rank_gloo(O, world):
+    """Column panels dealt over `world` processes, one broadcast of the
+    multipliers per block step, the remaining block gathered and ranked at
+    the end: every process returns the oracle's rank."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs)
+    out = {}
+    while not q.empty():
+        r, got = q.get()
+        out[r] = got
+    want = [O.rank(p, _case_matrix(O, kind, p, n, L), n) for kind, p, n, L in SHARD_CASES]
+    assert sorted(out) == list(range(world))
+    for r in range(world):
+        assert out[r] == want, (r, out[r], want)
