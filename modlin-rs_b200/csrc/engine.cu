@@ -60,6 +60,10 @@ struct Tune {
   int bm_threads[4] = {256, 256, 1024, 1024};       // n < 1024, < 4096, < 16384, longer
   int bm_cluster_min = 16384;
   int bm_batch_threads[3] = {128, 256, 512};        // longest < 512, < 2048, longer
+  // Shared memory per batch CTA (KiB), by the same classes: a sequence whose
+  // c, b, t (24 bytes per entry) do not fit runs from the CTA's global
+  // workspace; smaller caps put more CTAs on an SM.
+  int bm_batch_smem_kib[3] = {200, 200, 200};
   int batch_tc_min = 1 << 30;  // batched rank: sides on the tensor-core kernel (off until measured faster)
 };
 
@@ -710,7 +714,7 @@ static int lc_batch_locked(Ctx* C, const uint64_t* p, const uint64_t* const* d_d
   // Longest first: the persistent CTAs then finish close together (LPT).
   std::stable_sort(jobs.begin(), jobs.end(), [](const BmJob& a, const BmJob& b) { return a.n > b.n; });
   const int threads = C->tune.bm_batch_threads[bm_batch_class(maxn)];
-  int64_t smem_words = std::min<int64_t>(3 * maxn, (200 * 1024) / 8);
+  int64_t smem_words = std::min<int64_t>(3 * maxn, (int64_t)C->tune.bm_batch_smem_kib[bm_batch_class(maxn)] * 128);
   int per_sm = bm_batch_max_blocks_per_sm(threads, smem_words);
   if (per_sm < 1) per_sm = 1;
   int blocks = C->num_sms * per_sm;
@@ -957,7 +961,8 @@ static int autotune_locked(Ctx* C, std::string& rep) {
     T.bm_cluster_min = crossover(csz, cl_wins, 1 << 30);
   }
   rep += "}";
-  // 5. BM batches: threads per CTA by the longest sequence.
+  // 5. BM batches: threads per CTA and the shared-memory cap per CTA by the
+  //    longest sequence.
   {
     const int64_t lo[3] = {64, 512, 2048}, hi[3] = {512, 2048, 8192};
     const int bthr[3] = {128, 256, 512};
@@ -979,25 +984,32 @@ static int autotune_locked(Ctx* C, std::string& rep) {
         ptrs[i] = arena + (size_t)i * 8192;
       }
       float best = 1e30f;
-      const int saved = C->tune.bm_batch_threads[c];
-      for (int t : bthr) {
-        C->tune.bm_batch_threads[c] = t;
-        const float ms = best_ms(C, 1, [&]() -> int {
-          return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, out.data(), st);
-        }, &rc);
-        if (rc) {
-          C->tune.bm_batch_threads[c] = saved;
-          return rc;
-        }
-        std::snprintf(buf, sizeof buf, "%s\"max<%lld t=%d\": %.3f", rep.back() == '{' ? "" : ", ",
-                      (long long)hi[c], t, ms);
-        rep += buf;
-        if (ms < best) {
-          best = ms;
-          T.bm_batch_threads[c] = t;
+      const int saved = C->tune.bm_batch_threads[c], saved_kib = C->tune.bm_batch_smem_kib[c];
+      for (int kib : {200, 96, 48, 24}) {
+        if (kib < 200 && (int64_t)kib * 1024 >= 24 * hi[c]) continue;  // the same as a larger cap
+        for (int t : bthr) {
+          C->tune.bm_batch_threads[c] = t;
+          C->tune.bm_batch_smem_kib[c] = kib;
+          const float ms = best_ms(C, 1, [&]() -> int {
+            return lc_batch_locked(C, ps.data(), ptrs.data(), ns.data(), count, out.data(), st);
+          }, &rc);
+          if (rc) {
+            C->tune.bm_batch_threads[c] = saved;
+            C->tune.bm_batch_smem_kib[c] = saved_kib;
+            return rc;
+          }
+          std::snprintf(buf, sizeof buf, "%s\"max<%lld t=%d smem=%dK\": %.3f", rep.back() == '{' ? "" : ", ",
+                        (long long)hi[c], t, kib, ms);
+          rep += buf;
+          if (ms < best) {
+            best = ms;
+            T.bm_batch_threads[c] = t;
+            T.bm_batch_smem_kib[c] = kib;
+          }
         }
       }
       C->tune.bm_batch_threads[c] = saved;
+      C->tune.bm_batch_smem_kib[c] = saved_kib;
     }
     rep += "}";
   }
@@ -1006,10 +1018,11 @@ static int autotune_locked(Ctx* C, std::string& rep) {
   std::snprintf(buf, sizeof buf,
                 ", \"choice\": {\"tc_crossover\": [%d, %d, %d, %d], \"two_panel_min\": %d, "
                 "\"batch_tc_min\": %d, \"bm_threads\": [%d, %d, %d, %d], \"bm_cluster_min\": %d, "
-                "\"bm_batch_threads\": [%d, %d, %d]}}",
+                "\"bm_batch_threads\": [%d, %d, %d], \"bm_batch_smem_kib\": [%d, %d, %d]}}",
                 T.tc_cross[0], T.tc_cross[1], T.tc_cross[2], T.tc_cross[3], T.two_panel_min, T.batch_tc_min,
                 T.bm_threads[0], T.bm_threads[1], T.bm_threads[2], T.bm_threads[3], T.bm_cluster_min,
-                T.bm_batch_threads[0], T.bm_batch_threads[1], T.bm_batch_threads[2]);
+                T.bm_batch_threads[0], T.bm_batch_threads[1], T.bm_batch_threads[2], T.bm_batch_smem_kib[0],
+                T.bm_batch_smem_kib[1], T.bm_batch_smem_kib[2]);
   rep += buf;
   return MODLIN_OK;
 }
@@ -1651,7 +1664,7 @@ int modlin_lc_batch_plan_new(const uint64_t* p, const uint64_t* const* d_s, cons
   P->count = (int64_t)count;
   P->out = d_lcs_out;
   P->threads = C->tune.bm_batch_threads[bm_batch_class(maxn)];
-  P->smem_words = std::min<int64_t>(3 * maxn, (200 * 1024) / 8);
+  P->smem_words = std::min<int64_t>(3 * maxn, (int64_t)C->tune.bm_batch_smem_kib[bm_batch_class(maxn)] * 128);
   const int per_sm = std::max(1, bm_batch_max_blocks_per_sm(P->threads, P->smem_words));
   P->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)C->num_sms * per_sm, (int64_t)count));
   P->gws_words = 3 * maxn > P->smem_words ? 3 * maxn : 0;

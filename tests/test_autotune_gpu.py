@@ -14,6 +14,7 @@ def test_autotune_then_auto_paths_exact(M, O):
     assert len(ch["tc_crossover"]) == 4 and all(c >= 64 for c in ch["tc_crossover"])
     assert ch["bm_threads"] and all(t in (128, 256, 512, 1024) for t in ch["bm_threads"])
     assert all(t in (128, 256, 512) for t in ch["bm_batch_threads"])
+    assert all(k in (200, 96, 48, 24) for k in ch["bm_batch_smem_kib"])
     assert ch["bm_cluster_min"] >= 4096
     assert ch["two_panel_min"] in (0, 2048, 4096, 6144, 8192, 12288, 1 << 30)
     assert len(rep["two_panel_ms"]) == 7
