@@ -575,6 +575,26 @@ def prng_fill_measure(torch, modlin, count=1 << 32, host_sample=1 << 23, readme_
     return res
 
 
+def tc_update_schedule(n, two_panel_min):
+    """Trailing updates of a full-rank n x n rank on the tensor-core path:
+    two-panel steps (K = 128) while at least two_panel_min rows remain, then
+    one-panel steps (K = 64); returns (K = 128 updates, K = 64 updates, total
+    C outputs updated)."""
+    col, k128, k64, outs = 0, 0, 0, 0
+    while col < n:
+        if n - col >= two_panel_min and n - col >= 128:
+            if col + 128 < n:
+                k128 += 1
+                outs += (n - col - 128) ** 2
+            col += 128
+        else:
+            if col + 64 < n:
+                k64 += 1
+                outs += (n - col - 64) ** 2
+            col += 64
+    return k128, k64, outs
+
+
 def host_cores():
     try:
         import oracle
@@ -787,10 +807,13 @@ def main():
         peaks = measured_peaks()
         tr_ms = statistics.median(trailing_ms)
         Wtr = statistics.median(trailing_macs)
-        # Timed trailing updates per rank: one per two-panel step on the
-        # tensor-core path (K = 128), one per panel on the plain path.
-        depth = 128 if kernel == "tc" else 64
-        n_tr = sum(1 for _ in range(0, n, depth)) - 1
+        # Timed trailing updates per rank: one per block step on the
+        # tensor-core path (K = 128 while at least the tuned two_panel_min
+        # rows remain, the library default 256 without tuning; K = 64 after),
+        # one per panel on the plain path.
+        tpm = tune["two_panel_min"] if tune else 256
+        k128, k64, outs = tc_update_schedule(n, tpm)
+        n_tr = k128 + k64 if kernel == "tc" else sum(1 for _ in range(0, n, 64)) - 1
         per_launch_ms = tr_ms / max(n_tr, 1)
         if kernel == "tc":
             int8 = int8_peak_tops(torch)
@@ -804,7 +827,7 @@ def main():
             # the first wide K = 128 update of the 8192^2 rank was 550.0 + 454.4 MB
             # for 8064 x 7936 outputs (15.69 B per output against 16 algorithmic:
             # C read + write); scaled to this run's average launch by its outputs.
-            outputs_per_launch = Wtr / depth / max(n_tr, 1)
+            outputs_per_launch = outs / max(n_tr, 1)
             traffic = 15.69 * outputs_per_launch
             roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": traffic,
@@ -814,7 +837,7 @@ def main():
                     "kernel": "trailing_tc (tcgen05 kind::i8)",
                     "peak_source": peak_note,
                     "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops "
-                                              f"(K = {depth}, {n_tr} updates per rank)",
+                                              f"({k128} updates at K = 128, {k64} at K = 64 per rank)",
                     "avg_launch_ms": per_launch_ms}
         else:
             peak = peaks.get("hbm_gbs", 6650.0)
