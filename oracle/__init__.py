@@ -23,9 +23,22 @@ szp = ctypes.POINTER(ctypes.c_size_t)
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the committed Makefile (gcc, OpenMP)."""
+    if _SO != os.path.join(_HERE, "liboracle.so"):
+        return _SO
     if force or not os.path.exists(_SO) or _stale():
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _SO
+
+
+def use_native(path: str) -> str:
+    """Build the oracle with -march=native for the CPU this process runs on
+    (the reference's release builds use target-cpu=native) into `path`, and
+    load that library from now on. Must be called before the first use."""
+    global _SO
+    assert _lib is None, "use_native() must come before the oracle is loaded"
+    subprocess.run(["make", "-s", "-C", _HERE, "native", f"NATIVE_OUT={path}"], check=True)
+    _SO = path
+    return path
 
 
 def _stale() -> bool:
@@ -79,6 +92,9 @@ def lib():
         L.oracle_gen_uniform.argtypes = [ctypes.c_uint64, u64p, u64p, ctypes.c_size_t]
         L.oracle_gen_planted.restype = None
         L.oracle_gen_planted.argtypes = [ctypes.c_uint64, ctypes.c_size_t, u64p, u64p, ctypes.c_size_t]
+        L.oracle_gen_dependent.restype = None
+        L.oracle_gen_dependent.argtypes = [ctypes.c_uint64, ctypes.c_size_t, u64p, ctypes.c_size_t, ctypes.c_size_t,
+                                           u64p, szp]
         _lib = L
     return _lib
 
@@ -219,6 +235,18 @@ def gen_uniform(p: int, seed: int, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.uint64)
     lib().oracle_gen_uniform(p, ctypes.byref(st), out.ctypes.data_as(u64p), count)
     return out
+
+
+def gen_dependent(p: int, n: int, seed: int, ncols: int, nrows: int):
+    """n x n uniform matrix (SplitMix64(seed)) with `ncols` planted dependent
+    columns and its last `nrows` rows replaced by combinations of earlier
+    rows; returns (matrix as a flat array, sorted planted columns)."""
+    st = ctypes.c_uint64(seed)
+    out = np.zeros(n * n, dtype=np.uint64)
+    dep = np.zeros(max(ncols, 1), dtype=np.uint64)
+    lib().oracle_gen_dependent(p, n, ctypes.byref(st), ncols, nrows, out.ctypes.data_as(u64p),
+                               dep.ctypes.data_as(szp))
+    return out, [int(x) for x in dep[:ncols]]
 
 
 def gen_planted(p: int, L: int, seed: int, count: int) -> np.ndarray:

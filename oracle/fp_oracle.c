@@ -431,3 +431,73 @@ void oracle_gen_planted(uint64_t p, size_t L, uint64_t *state, uint64_t *out, si
     free(a);
     free(init);
 }
+
+/* Matrix with planted dependencies (checker input; no reference counterpart).
+ * An n x n matrix of uniform residues from `state` (row-major), then:
+ *  - ncols distinct columns j, drawn as splitmix64 % (n - 2) + 2 (redrawn when
+ *    already taken) and processed in increasing order, each become
+ *    a*col(j1) + b*col(j2) with j1 = splitmix64 % j, j2 = splitmix64 % j and
+ *    a, b uniform residues (drawn in that order per column);
+ *  - each of the last nrows rows becomes sum_{t<4} c_t * row(i_t) with
+ *    i_t = splitmix64 % (n - nrows) and c_t a uniform residue (drawn i_t, c_t
+ *    per term, rows in increasing order).
+ * Generically rank = n - max(ncols, nrows), and the pivot columns are the
+ * first `rank` columns outside the planted set. dep_cols (ncols entries)
+ * receives the planted columns in increasing order. */
+static int cmp_size(const void *x, const void *y) {
+    size_t a = *(const size_t *)x, b = *(const size_t *)y;
+    return a < b ? -1 : a > b;
+}
+
+void oracle_gen_dependent(uint64_t p, size_t n, uint64_t *state, size_t ncols, size_t nrows, uint64_t *out,
+                          size_t *dep_cols) {
+    oracle_field F;
+    oracle_field_new(p, &F);
+    oracle_gen_uniform(p, state, out, n * n);
+    if (n < 3) ncols = 0;
+    if (ncols > n - 2) ncols = n - 2;
+    if (nrows >= n) nrows = n - 1;
+    unsigned char *taken = (unsigned char *)calloc(n, 1);
+    for (size_t t = 0; t < ncols; t++) {
+        size_t j;
+        do j = (size_t)(oracle_splitmix64(state) % (n - 2)) + 2; while (taken[j]);
+        taken[j] = 1;
+        dep_cols[t] = j;
+    }
+    qsort(dep_cols, ncols, sizeof(size_t), cmp_size);
+    size_t *src = (size_t *)malloc((2 * ncols + 1) * sizeof(size_t));
+    uint64_t *cf = (uint64_t *)malloc((2 * ncols + 1) * sizeof(uint64_t));
+    for (size_t t = 0; t < ncols; t++) {
+        const size_t j = dep_cols[t];
+        src[2 * t] = (size_t)(oracle_splitmix64(state) % j);
+        src[2 * t + 1] = (size_t)(oracle_splitmix64(state) % j);
+        cf[2 * t] = uniform_residue(p, state);
+        cf[2 * t + 1] = uniform_residue(p, state);
+    }
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n; i++) {
+        uint64_t *r = out + i * n;
+        for (size_t t = 0; t < ncols; t++)
+            r[dep_cols[t]] = f_add(&F, f_mul(&F, cf[2 * t], r[src[2 * t]]), f_mul(&F, cf[2 * t + 1], r[src[2 * t + 1]]));
+    }
+    size_t *rs = (size_t *)malloc((4 * nrows + 1) * sizeof(size_t));
+    uint64_t *rc = (uint64_t *)malloc((4 * nrows + 1) * sizeof(uint64_t));
+    for (size_t t = 0; t < 4 * nrows; t++) {
+        rs[t] = (size_t)(oracle_splitmix64(state) % (n - nrows));
+        rc[t] = uniform_residue(p, state);
+    }
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < nrows; q++) {
+        uint64_t *r = out + (n - nrows + q) * n;
+        for (size_t c = 0; c < n; c++) {
+            uint64_t v = 0;
+            for (int t = 0; t < 4; t++) v = f_add(&F, v, f_mul(&F, rc[4 * q + t], out[rs[4 * q + t] * n + c]));
+            r[c] = v;
+        }
+    }
+    free(taken);
+    free(src);
+    free(cf);
+    free(rs);
+    free(rc);
+}

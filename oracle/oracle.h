@@ -94,6 +94,10 @@ void oracle_test_lc_lfsr(uint64_t p, size_t k, size_t len, uint64_t *seed, uint6
  * order-L recurrences), used to cross-check the product's generators. */
 void oracle_gen_uniform(uint64_t p, uint64_t *state, uint64_t *out, size_t count);
 void oracle_gen_planted(uint64_t p, size_t L, uint64_t *state, uint64_t *out, size_t count);
+/* n x n uniform matrix with ncols columns and the last nrows rows replaced by
+ * combinations of earlier ones (checker input for full-size parity tests). */
+void oracle_gen_dependent(uint64_t p, size_t n, uint64_t *state, size_t ncols, size_t nrows, uint64_t *out,
+                          size_t *dep_cols);
 
 #ifdef __cplusplus
 }
