@@ -34,7 +34,7 @@ extern "C" {
 
 #define MODLIN_OK 0
 #define MODLIN_EINVAL_P (-1)   /* p < 2 or p >= 2^63 (src/fp.rs:50-51) */
-#define MODLIN_EINVAL_N (-2)   /* n == 0 or n*n overflows / exceeds the device limit */
+#define MODLIN_EINVAL_N (-2)   /* rank of n == 0, n*n overflows, or n exceeds a limit */
 #define MODLIN_EINPUT (-3)     /* an entry is >= p (checked only on request) */
 #define MODLIN_ECUDA (-4)      /* CUDA runtime error */
 #define MODLIN_ENOMEM (-5)     /* device or host allocation failed */
@@ -147,12 +147,16 @@ int modlin_linear_complexity_device(uint64_t p, const uint64_t *d_s, size_t n,
  * memory on the call path (a host whose pool allocator owns all device
  * memory, or a loop that must not pay cudaMalloc's implicit synchronisation):
  * the linear complexity of the device sequence d_s[0..n) is written to the
- * device slot *d_lc_out, asynchronously on `stream`, without any allocation.
- * The Berlekamp-Massey scratch lives in a fixed 6 MiB device array, so
- * n <= 262144 (MODLIN_EINVAL_N beyond). All calls share that array: calls
- * that overlap on the GPU race, so order them (e.g. one stream). The first
- * call on a device looks up the array's address; make it before any stream
- * capture. */
+ * device slot *d_lc_out, asynchronously on `stream`, without any allocation
+ * (n = 0 writes 0). The Berlekamp-Massey scratch lives in shared memory when
+ * it fits (n <= 8533), else in a fixed 6 MiB device array, so n <= 262144
+ * (MODLIN_EINVAL_N beyond). All calls share that array: calls that overlap on
+ * the GPU race, so order them (e.g. one stream). The first call on a device
+ * is a set-up that loads the library's device code for this entry point and
+ * the array (the CUDA driver allocates device memory for them) and looks up
+ * the array's address: make it (n = 0 is enough) before the caller's pool
+ * reserves the device memory and before any stream capture. Not usable on a
+ * device after cudaDeviceReset of that device. */
 int modlin_linear_complexity_device_noalloc(uint64_t p, const uint64_t *d_s, size_t n,
                                             int64_t *d_lc_out, void *stream);
 
@@ -287,6 +291,13 @@ int modlin_autotune(char *report, size_t cap);
 /* Number of this library's kernel launches since load (for launch-count
  * claims in measurements). */
 uint64_t modlin_kernel_launches(void);
+/* Failure-detection test hook (no reference counterpart; the reference has
+ * no device waits): the next MODLIN_LC_GRID launch in this process bounds
+ * each grid-barrier wait by spin_cycles (1 .. 4e9) instead of ~1 s, and its
+ * CTA skip_cta (a CTA the launch has: 0 always is) does not arrive at the
+ * first step's barrier, so every wait expires, the kernel returns early and
+ * the call reports MODLIN_ETIMEOUT. Nothing faults or hangs. */
+int modlin_testing_grid_timeout_once(long long spin_cycles, int skip_cta);
 /* Milliseconds spent in the trailing-update kernels of the last rank call,
  * measured with CUDA events on the launching stream (0 if unavailable). */
 double modlin_last_trailing_ms(void);

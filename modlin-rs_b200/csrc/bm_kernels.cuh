@@ -23,8 +23,15 @@ cudaError_t launch_bm_batch(const BmJob* d_jobs, int64_t count, unsigned long lo
                             int64_t gws_words, int64_t smem_words, int blocks, int threads, int64_t* d_out,
                             cudaStream_t st);
 int bm_batch_max_blocks_per_sm(int threads, int64_t smem_words);
+// Loads the module of bm_block_kernel on the current device now (a lazily
+// loaded module would otherwise be loaded, and its memory allocated, at the
+// first launch).
+cudaError_t bm_block_prepare();
+// spin: cycles a CTA waits at a grid barrier before it gives up and sets the
+// error word; skip_cta (>= 0, tests only): that CTA skips its arrival at the
+// first step barrier, so the waits expire.
 cudaError_t launch_bm_grid(const FieldParams& fp, const uint64_t* s, int64_t n, int ctas, int threads, uint64_t* b0,
-                           uint64_t* b1, void* gs, long long spin, int64_t* d_out, cudaStream_t st,
+                           uint64_t* b1, void* gs, long long spin, int skip_cta, int64_t* d_out, cudaStream_t st,
                            int* ctas_used);
 // One long sequence on one thread-block cluster of R = 16 CTAs (8 where 16
 // cannot be launched and the slices fit); b0, b1: n-word global workspaces.

@@ -25,6 +25,11 @@
 namespace modlin {
 
 std::atomic<uint64_t> g_launches{0};
+// Failure-detection test (modlin_testing_grid_timeout_once): the next grid
+// Berlekamp-Massey launch waits at most g_fault_spin cycles per barrier and
+// CTA g_fault_skip_cta skips its first step arrival; consumed by that launch.
+static std::atomic<long long> g_fault_spin{0};
+static std::atomic<int> g_fault_skip_cta{-1};
 static double g_last_trailing_ms = 0.0;
 static double g_last_trailing_macs = 0.0;
 
@@ -610,8 +615,10 @@ static int lc_device_locked(Ctx* C, uint64_t p, const uint64_t* d_s, size_t n, c
     uint64_t* b0 = C->bmws.as<uint64_t>();
     int used = 0;
     // About one second of spinning at ~2 GHz before a wait is declared stuck.
-    const long long spin = 2000000000LL;
-    CK(launch_bm_grid(fp, d_s, (int64_t)n, ctas, 256, b0, b0 + n, C->bmsync.p, spin, d_out, st, &used));
+    long long spin = 2000000000LL;
+    const int skip_cta = g_fault_skip_cta.exchange(-1);
+    if (skip_cta >= 0) spin = g_fault_spin.load();
+    CK(launch_bm_grid(fp, d_s, (int64_t)n, ctas, 256, b0, b0 + n, C->bmsync.p, spin, skip_cta, d_out, st, &used));
     g_launches += 2;
     int err = 0;
     CK(cudaMemcpyAsync(&err, C->bmsync.as<char>() + grid_sync_err_offset(), sizeof(int), cudaMemcpyDeviceToHost,
@@ -1551,6 +1558,13 @@ int modlin_rank_prng(uint64_t p, modlin_prng* g, size_t n, const modlin_rank_opt
 }
 
 uint64_t modlin_kernel_launches(void) { return g_launches.load(); }
+
+int modlin_testing_grid_timeout_once(long long spin_cycles, int skip_cta) {
+  if (spin_cycles < 1 || spin_cycles > 4000000000LL || skip_cta < 0) return MODLIN_EINVAL_ARG;
+  g_fault_spin.store(spin_cycles);
+  g_fault_skip_cta.store(skip_cta);
+  return MODLIN_OK;
+}
 
 double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
 

@@ -227,3 +227,11 @@ def test_mixmax_folds_keep_p_for_zero(M, kind):
     out = g.fill(2 * (N - 1))
     p3 = np.uint64((M61 << 3) & ((1 << 64) - 1))
     assert out[4] == p3 and out[N - 1 + N - 2] == p3
+
+
+def test_timeout_hook_rejects_bad_arguments(M):
+    """The failure-detection hook validates its arguments on the host."""
+    L = M.lib()
+    assert L.modlin_testing_grid_timeout_once(0, 0) == -8
+    assert L.modlin_testing_grid_timeout_once(1000, -1) == -8
+    assert L.modlin_testing_grid_timeout_once(5_000_000_000, 0) == -8
