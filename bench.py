@@ -124,6 +124,44 @@ def measured_peaks():
         return {}
 
 
+def golden_configs():
+    """The CPU oracle's answers on these workloads at full size
+    (tests/golden/configs.json.gz, written by tests/golden/make_config_golden.py);
+    {} when the file is absent."""
+    import gzip
+    try:
+        with gzip.open(os.path.join(ROOT, "tests", "golden", "configs.json.gz"), "rt") as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def sha256_device(t, chunk=1 << 25):
+    """SHA-256 of a device int64 tensor's little-endian bytes (host copies in chunks)."""
+    import hashlib
+    h = hashlib.sha256()
+    flat = t.reshape(-1)
+    for i in range(0, flat.numel(), chunk):
+        h.update(flat[i:i + chunk].cpu().numpy().tobytes())
+    return h.hexdigest()
+
+
+def sha256_u64(values):
+    import hashlib
+    import numpy as np
+    return hashlib.sha256(np.array(values, dtype=np.uint64).tobytes()).hexdigest()
+
+
+def arena_digest(arena, ptrs, counts):
+    """Checksum of checksums of a batch arena: SHA-256 of the concatenated
+    per-job SHA-256 digests, jobs in order (the oracle's input checksum)."""
+    import hashlib
+    host = arena.cpu().numpy()
+    base = ptrs[0]
+    parts = [hashlib.sha256(host[(p - base) // 8:(p - base) // 8 + c].tobytes()).digest() for p, c in zip(ptrs, counts)]
+    return hashlib.sha256(b"".join(parts)).hexdigest()
+
+
 def int8_peak_tops(torch):
     """Dense INT8 tensor throughput on this GPU: cuBLASLt int8 GEMM via
     torch._int_mm (best of 5, 8192^3). None when unavailable."""
@@ -243,6 +281,7 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     threaded algorithm) on bounded samples of both."""
     from modlin import fp as mfp
     res = {}
+    gold = golden_configs()
     for name, planted, seed in (("long_planted", True, 21), ("long_iid", False, 22)):
         t = torch.empty(long_n, dtype=torch.int64, device="cuda")
         if planted:
@@ -251,6 +290,10 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
             modlin.gen.uniform_device(M61, seed, t.data_ptr(), long_n)
         torch.cuda.synchronize()
         entry = {"n": long_n, "expected": long_L if planted else "about n/2"}
+        g = gold.get(f"lc_{'planted' if planted else 'iid'}_{long_n}")
+        if g:
+            assert sha256_device(t) == g["input_sha256"], name
+            entry["oracle"] = {"lc": g["lc"], "macs": g["dot_macs"] + g["axpy_macs"], "input_sha256_equal": True}
         # The default (one 16-CTA cluster) and the whole-grid kernel.
         for kern in ("cluster", "grid"):
             for _ in range(warmup):
@@ -264,8 +307,12 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
             ms = e0.elapsed_time(e1) / steps
             if planted:
                 assert lc == long_L, (lc, long_L)
+            if g:
+                assert lc == g["lc"], (name, kern, lc, g["lc"])
             entry["lc"] = lc
             entry[kern] = {"ms": ms, "steps_per_s": long_n / (ms * 1e-3), "us_per_step": 1e3 * ms / long_n}
+            if g:
+                entry[kern]["mac_per_s"] = (g["dot_macs"] + g["axpy_macs"]) / (ms * 1e-3)
         entry["steps_per_s"] = entry["cluster"]["steps_per_s"]
         res[name] = entry
         del t
@@ -288,6 +335,14 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     iid_dev = max(abs(lcs[i] - (j[1] + 1) // 2) for i, j in enumerate(jobs) if not j[2])
     batch = {"sequences": len(jobs), "total_steps": total, "ms": ms, "steps_per_s": total / (ms * 1e-3),
              "planted_exact": True, "iid_max_dev_from_half": iid_dev}
+    g = gold.get(f"lc_batch_{len(jobs)}")
+    if g:
+        assert arena_digest(arena, ptrs, ns) == g["input_sha256_of_job_sha256"]
+        wrong = [i for i in range(len(jobs)) if lcs[i] != g["lcs"][i]]
+        assert not wrong, wrong[:5]
+        batch["oracle"] = {"all_lcs_equal": True, "sequences_compared": len(jobs), "input_digest_equal": True,
+                           "macs": g["macs"]}
+        batch["mac_per_s"] = g["macs"] / (ms * 1e-3)
     # Plain form: one sequence per launch, each call waits for its result.
     idx = list(range(0, len(jobs), max(1, len(jobs) // plain_sample)))[:plain_sample]
     sub = sum(ns[i] for i in idx)
@@ -340,13 +395,14 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
         steps_cpu = sum(ns[i] for i in sample)
         batch["cpu_oracle_one_thread"] = {"sequences": len(sample), "steps": steps_cpu, "s": dt,
                                           "steps_per_s": steps_cpu / dt}
-        nl = 40000
-        t = modlin.gen.uniform(M61, 22, nl)
+        # The whole n = 200000 iid sequence (about a minute on one core).
+        t = modlin.gen.uniform(M61, 22, long_n)
         t0 = time.perf_counter()
-        oracle.linear_complexity(M61, t)
+        lc_cpu = oracle.linear_complexity(M61, t)
         dt = time.perf_counter() - t0
-        res["long_iid"]["cpu_oracle_one_thread"] = {"n": nl, "s": dt, "steps_per_s": nl / dt,
-                                                    "note": "prefix of length 40000 of the same stream"}
+        assert lc_cpu == res["long_iid"]["lc"]
+        res["long_iid"]["cpu_oracle_one_thread"] = {"n": long_n, "s": dt, "steps_per_s": long_n / dt,
+                                                    "note": "the whole sequence, one thread (as the reference)"}
     res["batch"] = batch
     del arena
     return res
@@ -431,28 +487,20 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    # Generic ranks: n (iid) and L (planted). Over small primes a few
-    # matrices are singular / rank-deficient by chance; those are checked
-    # against the oracle, whose column profile also gives their exact work.
+    # Every rank against the oracle's (tests/golden/configs.json.gz), whose
+    # column profiles also give the batch's exact modMAC work.
+    g = golden_configs().get(f"rank_batch_{len(jobs)}")
+    assert g, "no cached oracle answers for this batch"
+    assert arena_digest(pristine, pptrs, [n * n for n in ns]) == g["input_sha256_of_job_sha256"]
+    wrong = [i for i in range(len(jobs)) if ranks[i] != g["ranks"][i]]
+    assert not wrong, wrong[:5]
+    work_mac = g["work_modmac"]
     want = [j[3] if j[2] else j[1] for j in jobs]
-    mism = [i for i in range(len(jobs)) if ranks[i] != want[i]]
-    pcols = {i: range(ranks[i]) for i in range(len(jobs))}
-    confirmed = 0
-    if mism:
-        import oracle
-        oracle.build()
-        for i in mism:
-            n = ns[i]
-            a = pristine[(pptrs[i] - pptrs[0]) // 8:(pptrs[i] - pptrs[0]) // 8 + n * n].cpu().numpy().view("uint64")
-            r, pc = oracle.rank(ps[i], a, n, with_pcols=True)
-            confirmed += r == ranks[i]
-            pcols[i] = pc
-    work_mac = sum(sum((ns[i] - 1 - k) * (ns[i] - 1 - j) for k, j in enumerate(pcols[i])) for i in range(len(jobs)))
     res = {"matrices": len(jobs), "ms": ms, "matrices_per_s": len(jobs) / (ms * 1e-3), "work_modmac": work_mac,
-           "modmac_per_s": work_mac / (ms * 1e-3), "non_generic_ranks": len(mism),
-           "non_generic_ranks_equal_to_oracle": confirmed,
+           "modmac_per_s": work_mac / (ms * 1e-3),
+           "oracle": {"all_ranks_equal": True, "matrices_compared": len(jobs), "input_digest_equal": True,
+                      "non_generic_ranks": sum(1 for i in range(len(jobs)) if ranks[i] != want[i])},
            "step": "restore the 4096 matrices from a pristine copy + one batched call"}
-    assert confirmed == len(mism)
     # The same batch as a plan captured in a CUDA graph: each replay restores
     # the matrices and ranks them all (one copy, one counter reset, one
     # persistent launch; no host synchronisation inside).
@@ -509,10 +557,17 @@ def rank_planted_measure(torch, modlin, n=16384, L=4096, seed=8, steps=1):
     work = torch.empty_like(pristine)
     W = sum((n - 1 - k) ** 2 for k in range(L))
     res = {"n": n, "order": L, "work_modmac": W, "generation_s": gen_s}
+    g = golden_configs().get(f"rank_planted_{n}")
+    if g:
+        assert sha256_device(pristine) == g["input_sha256"]
+        assert g["rank"] == L and g["work_modmac"] == W
     for kern in ("tc", "plain"):
         work.copy_(pristine)
         r, pc = mfp.rank_device(M61, work.data_ptr(), n, kernel=kern, pivot_cols=True)
         assert r == L and list(pc) == list(range(L)), (kern, r)
+        if g:
+            assert sha256_u64(pc) == g["pcols_sha256"]
+            res["oracle"] = {"rank": g["rank"], "pcols_equal": True, "input_sha256_equal": True}
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ms = 0.0
         for _ in range(steps):
@@ -719,6 +774,16 @@ def main():
 
     r, pcols = step(kernel, True)
     W = algorithmic_work(n, pcols)
+    # The oracle's answer for this matrix (computed once on the CPU, cached
+    # with the input's SHA-256): same input, same rank, same pivot columns.
+    parity = {"oracle": "no cached answer for this size"}
+    g = golden_configs().get(f"rank_uniform_{n}")
+    if g and rank == 0:
+        assert sha256_device(pristine) == g["input_sha256"], "input differs from the oracle's"
+        assert r == g["rank"], (r, g["rank"])
+        assert sha256_u64(pcols) == g["pcols_sha256"]
+        parity = {"oracle": "rank and pivot columns equal the CPU oracle's on the same input (SHA-256 checked)",
+                  "oracle_rank": g["rank"], "oracle_work_modmac": g["work_modmac"]}
     Wtr = trailing_work(n, pcols)
     for _ in range(args.warmup):
         step(kernel)
@@ -868,7 +933,7 @@ def main():
                        "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                        "l2": "inputs (2 GiB) larger than L2", "rank": r, "work_modmac": W,
                        "autotuned": tune},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "parity": parity,
             "clocks": clk.summary(), **extras,
         }
         print(json.dumps(line), flush=True)
