@@ -72,6 +72,11 @@ struct Shape {
   static constexpr int C_BYTES = LIMBS == 8 ? CDEPTH * 128 * kCStride * 8 : 0;  // staged C tiles
   static constexpr int SMEM = A_BYTES + STAGES * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
   static_assert(SMEM <= 227 * 1024, "shared memory");
+  // p = 2^61 - 1: the epilogue keeps C in registers, so the shared memory of
+  // the staged C tiles goes to a deeper B ring.
+  static constexpr int STAGES_M61 = KK == 64 ? 8 : 5;
+  static constexpr int SMEM_M61 = A_BYTES + STAGES_M61 * B_BYTES + ZERO_BYTES + 1024;
+  static_assert(SMEM_M61 <= 227 * 1024, "shared memory");
 };
 
 struct Sched {
@@ -157,13 +162,46 @@ __device__ __forceinline__ uint64_t finish(const F& f, u128 lo, u128 hi, uint64_
   }
 }
 
+__device__ __forceinline__ uint64_t mad_wide_u32(uint32_t a, uint32_t b, uint64_t c) {
+  uint64_t d;
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+  return d;
+}
+
+// x = sum_{d<15} 2^(8d) a[d][c] mod 2^61 - 1, lazily: x < 2^62 and congruent.
+// The diagonal sums are a[d][c] <= 8 * 128 * 255^2 < 2^26 (K <= 128), and
+// 2^(8(d+8)) = 8 * 2^(8d) (mod p), so V_d = a_d + 8 a_(d+8) <= 57 * 128 * 255^2
+// < 2^29 (d < 7; V_7 = a_7). L = sum_{d<4} 2^(8d) V_d and H = sum_{d<4}
+// 2^(8d) V_(d+4) are < 2^54, and 2^32 H = 2^32 (H mod 2^29) + (H >> 29) (mod p)
+// since 2^61 = 1, so x = L + 2^32 (H mod 2^29) + (H >> 29) < 2^62.
+__device__ __forceinline__ uint64_t m61_fold15(const uint32_t (&a)[15][4], int c) {
+  uint32_t V[8];
+#pragma unroll
+  for (int d = 0; d < 7; ++d) V[d] = a[d][c] + 8u * a[d + 8][c];
+  V[7] = a[7][c];
+  const uint64_t L = mad_wide_u32(V[3], 1u << 24, mad_wide_u32(V[2], 1u << 16, mad_wide_u32(V[1], 1u << 8, V[0])));
+  const uint64_t H = mad_wide_u32(V[7], 1u << 24, mad_wide_u32(V[6], 1u << 16, mad_wide_u32(V[5], 1u << 8, V[4])));
+  return L + ((uint64_t)((uint32_t)H & 0x1FFFFFFFu) << 32) + (H >> 29);
+}
+
+// (cv - x) mod 2^61 - 1 for a canonical cv and any x < 2^62:
+// y = cv + 4p - x lies in (0, 2^64), one fold leaves y1 <= p + 7, and one
+// conditional subtraction makes it canonical.
+__device__ __forceinline__ uint64_t m61_sub_lazy(uint64_t cv, uint64_t x) {
+  const uint64_t y = cv + (4 * kM61) - x;
+  const uint64_t y1 = (y & kM61) + (y >> 61);
+  return y1 >= kM61 ? y1 - kM61 : y1;
+}
+
 template <class F, int LIMBS, int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
                        int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err) {
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
-  constexpr int kStages = SH::STAGES;
+  // p = 2^61 - 1: two epilogue groups of 8 warps, one per accumulator buffer.
+  constexpr bool kM61Path = std::is_same<F, FpM61>::value;
+  constexpr int kStages = kM61Path ? SH::STAGES_M61 : SH::STAGES;
   constexpr int kCDepth = SH::CDEPTH;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sA = smem;                        // A_BYTES
@@ -188,7 +226,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(a_empty, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(acc_full + b, 1);
-      mbar_init(acc_empty + b, kEpiWarps);
+      mbar_init(acc_empty + b, kM61Path ? kEpiWarps / 2 : kEpiWarps);
     }
     mbar_init(mma_done, 1);
     for (int st = 0; st < kStages; ++st) {
@@ -280,6 +318,92 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_wait(mma_done, 0, err + 1);
     }
     __syncwarp();
+  } else if constexpr (kM61Path) {
+    // ---------------- epilogue, p = 2^61 - 1 ----------------------------------
+    // Two groups of 8 warps: group g drains accumulator buffer g, i.e. the
+    // subtiles it = g, g + 2, ... of this CTA's range, so each group has two
+    // MMA periods per subtile and the groups' phases interleave. In a group,
+    // warp w reads TMEM lanes 32*(w%4)..+32 (its 32 rows) and one half (8
+    // columns) of the 16-column subtile; every thread owns one row x 8
+    // columns: it loads their C values from global memory one subtile ahead
+    // (into registers), folds the 15 diagonal sums of each column, releases
+    // the buffer, and stores C - T. No shared memory, no barriers between
+    // warps.
+    const int ew = warp - 2;
+    const int grp = ew >> 3;          // accumulator buffer this group drains
+    const int quad = warp & 3;        // TMEM lane quadrant
+    const int half = (ew >> 2) & 1;   // column half of the subtile
+    const int row = quad * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + grp * 256 + half * 8;
+    const bool vec = (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0;
+    const int64_t nsub = S.nsub;
+    // Subtile it = grp + 2 k of [g0, g1): (mt, sb) tracked incrementally.
+    int64_t g = g0 + grp;
+    int64_t mt = g / nsub, sb = g - mt * nsub;
+    auto advance = [&]() {
+      g += 2;
+      sb += 2;
+      while (sb >= nsub) {
+        sb -= nsub;
+        ++mt;
+      }
+    };
+    auto load_c = [&](uint64_t (&cv)[8]) {
+      const int64_t r = (int64_t)rbeg + mt * 128 + row;
+      const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
+      const uint64_t* src = m + r * ld + c0;
+      if (r < rend && vec && c0 + 8 <= cend) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2*>(src) + q);
+          cv[2 * q] = v.x;
+          cv[2 * q + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) cv[c] = (r < rend && c0 + c < cend) ? __ldcs(src + c) : 0;
+      }
+    };
+    uint64_t cv[8];
+    if (g < g1) load_c(cv);
+    bool ok = true;
+    for (int k = 0; g < g1; ++k) {
+      if (!(ok = __all_sync(0xffffffffu, mbar_wait(acc_full + grp, k & 1, err)))) break;
+      fence_after();
+      uint64_t x[8];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        uint32_t a[15][4];
+#pragma unroll
+        for (int d = 0; d < 15; ++d) tmem_ld4(lane_base + d * NS + q * 4, a[d]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x[4 * q + c] = m61_fold15(a, c);
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty + grp);
+      const int64_t r = (int64_t)rbeg + mt * 128 + row;
+      const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
+      uint64_t res[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) res[c] = m61_sub_lazy(cv[c], x[c]);
+      uint64_t* dst = m + r * ld + c0;
+      if (r < rend) {
+        if (vec && c0 + 8 <= cend) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            __stcs(reinterpret_cast<ulonglong2*>(dst) + q, make_ulonglong2(res[2 * q], res[2 * q + 1]));
+        } else {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c0 + c < cend) dst[c] = res[c];
+        }
+      }
+      advance();
+      if (g < g1) load_c(cv);
+    }
+    if (!ok) atomicExch(err, 1);
   } else {
     // ---------------- epilogue: TMEM -> exact residue -> C -= T -------------
     // kEpiWarps warps: warp w reads TMEM lanes 32*(w%4)..+32 (its rows) and
@@ -367,37 +491,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (ok) {
           fence_after();
           uint64_t res[4];
-          if constexpr (std::is_same<F, FpM61>::value) {
-            uint32_t a[15][4];
-#pragma unroll
-            for (int d = 0; d < 15; ++d) tmem_ld4(lane_addr + d * NS, a[d]);
-            tmem_wait_ld();
-#pragma unroll
-            for (int d = 0; d < 15; ++d)
-#pragma unroll
-              for (int c = 0; c < 4; ++c) asm volatile("" : "+r"(a[d][c]));
-            fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acc_empty + ab);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              // 2^(8(d+8)) = 8 * 2^(8d) mod 2^61-1: V_d = S_d + 8 S_(d+8) < 2^29.
-              uint32_t V[8];
-#pragma unroll
-              for (int d = 0; d < 7; ++d) V[d] = a[d][c] + 8u * a[d + 8][c];
-              V[7] = a[7][c];
-              // u32 x u32 + u64 multiply-adds (one IMAD.WIDE each).
-              const uint64_t W0 = (uint64_t)V[3] * 16777216u +
-                                  ((uint64_t)V[2] * 65536u + ((uint64_t)V[1] * 256u + (uint64_t)V[0]));
-              const uint64_t W1 = (uint64_t)V[7] * 16777216u +
-                                  ((uint64_t)V[6] * 65536u + ((uint64_t)V[5] * 256u + (uint64_t)V[4]));
-              // W0 + 2^32 W1 mod p, with 2^32 W1 = ((W1 mod 2^29) << 32) + (W1 >> 29) mod p.
-              uint64_t x = W0 + ((uint64_t)((uint32_t)W1 & 0x1FFFFFFFu) << 32) + (W1 >> 29);  // < 2^62
-              x = (x & kM61) + (x >> 61);
-              x = x >= kM61 ? x - kM61 : x;
-              res[c] = cv[c] >= x ? cv[c] - x : cv[c] + kM61 - x;
-            }
-          } else {
+          {
             u128 lo[4], hi[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) lo[c] = hi[c] = 0;
@@ -542,13 +636,14 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
   S.nsub = (cend - jend + SH::NS - 1) / SH::NS;
   const int64_t total = (int64_t)S.mtiles * S.nsub;
   const int grid = total < max_ctas ? (int)total : max_ctas;  // one CTA per SM: it owns all 512 TMEM columns
+  constexpr int smem = std::is_same<F, FpM61>::value ? SH::SMEM_M61 : SH::SMEM;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
+    cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
-  trailing_tc_kernel<F, LIMBS, KK><<<grid, kThreads, SH::SMEM, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64,
-                                                                      err);
+  trailing_tc_kernel<F, LIMBS, KK><<<grid, kThreads, smem, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64,
+                                                                  err);
 }
 
 // (limb count, K tile) of a prime and an update depth.
