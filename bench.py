@@ -584,6 +584,65 @@ def rank_planted_measure(torch, modlin, n=16384, L=4096, seed=8, steps=1):
     return res
 
 
+def trailing_measure(torch, modlin, n=N, reps=3):
+    """The trailing update alone, both kernels on the same shape: the first
+    update of an n x n rank, C[(n-128) x (n-128)] -= L * U over 2^61-1
+    (src/fp.rs:202-248), uniform residues. K = 64 (one panel: the plain
+    kernel's depth) for both, and K = 128 (the two-panel depth the
+    tensor-core rank uses) on the tensor cores, against two K = 64 plain
+    updates. Each figure is the best of `reps` CUDA-event timings of
+    modlin_trailing_update_device (the tensor-core time includes its limb
+    splits). Also the plain kernel's roofline (modlin_plain_mac_peak: its
+    inner loop with no global traffic) and the plain kernel's fraction of it."""
+    from modlin import fp as mfp
+    M = n - 128
+    C = torch.empty(M * M, dtype=torch.int64, device="cuda")
+    L128 = torch.empty(M * 128, dtype=torch.int64, device="cuda")
+    U = torch.empty(128 * M, dtype=torch.int64, device="cuda")
+    modlin.gen.uniform_device(M61, 71, C.data_ptr(), M * M)
+    modlin.gen.uniform_device(M61, 72, L128.data_ptr(), M * 128)
+    modlin.gen.uniform_device(M61, 73, U.data_ptr(), 128 * M)
+    L64 = L128.view(M, 128)[:, :64].contiguous()
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    def upd(L, K, kern):
+        return lambda: mfp.trailing_update_device(M61, C.data_ptr(), M, M, M, L.data_ptr(), U.data_ptr(), M, K,
+                                                  kernel=kern)
+    res = {"shape": f"C {M}x{M} -= L {M}xK * U Kx{M} over 2^61-1", "ms": {}}
+    res["ms"]["plain_k64"] = timed(upd(L64, 64, "plain"))
+    res["ms"]["tc_k64"] = timed(upd(L64, 64, "tc"))
+    res["ms"]["tc_k128"] = timed(upd(L128, 128, "tc"))
+    macs64 = M * M * 64
+    rate = {k: (macs64 * (2 if k.endswith("128") else 1)) / (v * 1e-3) for k, v in res["ms"].items()}
+    res["modmac_per_s"] = rate
+    res["plain_trailing_modmac_per_s"] = rate["plain_k64"]
+    res["tc_trailing_modmac_per_s"] = rate["tc_k128"]
+    res["tc_vs_plain_same_shape_k64"] = rate["tc_k64"] / rate["plain_k64"]
+    res["tc_vs_plain"] = rate["tc_k128"] / rate["plain_k64"]
+    peak = mfp.plain_mac_peak(M61)
+    res["plain_mac_peak_modmac_per_s"] = peak
+    res["int_pipe_frac"] = rate["plain_k64"] / peak
+    res["roofline_plain"] = {"bound": "integer pipes", "achieved": rate["plain_k64"], "peak": peak,
+                             "unit": "modMAC/s", "frac": rate["plain_k64"] / peak,
+                             "peak_source": "measured: the plain kernel's inner loop alone (modlin_plain_mac_peak)"}
+    del C, L128, L64, U
+    torch.cuda.empty_cache()
+    return res
+
+
 def prng_fill_measure(torch, modlin, count=1 << 32, host_sample=1 << 23, readme_side=65536):
     """The generators' device fill (modlin_prng_fill_device) of the README's
     largest job, 2^32 outputs reduced mod 2^61-1 (a 65536^2 matrix), for
@@ -709,7 +768,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default AUTO choices")
-    ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch", "rank-planted"],
+    ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch", "rank-planted", "trailing"],
                     help="rank: the 16384^2 rank (default line); bm / rank-batch: only those measurements")
     args = ap.parse_args()
 
@@ -742,6 +801,11 @@ def main():
         res = rank_planted_measure(torch, modlin, steps=args.steps)
         if rank == 0:
             print(json.dumps({"workload": "planted large rank", **res}), flush=True)
+        return
+    if args.workload == "trailing":
+        res = trailing_measure(torch, modlin, n=args.n, reps=args.steps)
+        if rank == 0:
+            print(json.dumps({"workload": "trailing update", **res}), flush=True)
         return
     if args.workload == "rank-batch":
         res = rank_batch_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
@@ -830,6 +894,11 @@ def main():
             torch.cuda.synchronize()
             extras["plain_modmac_per_s"] = W / (e0.elapsed_time(e1) * 1e-3)
             extras["tc_speedup_vs_plain"] = value / world / extras["plain_modmac_per_s"]
+        # The trailing update alone: both kernels on the same shape.
+        extras["trailing_update"] = trailing_measure(torch, modlin)
+        extras["plain_trailing_modmac_per_s"] = extras["trailing_update"]["plain_trailing_modmac_per_s"]
+        extras["tc_trailing_modmac_per_s"] = extras["trailing_update"]["tc_trailing_modmac_per_s"]
+        extras["tc_vs_plain_trailing"] = extras["trailing_update"]["tc_vs_plain"]
         # Berlekamp-Massey: the long sequences and the 65536-sequence batch.
         extras["berlekamp_massey"] = bm_measure(torch, modlin, steps=1, warmup=1, plain_sample=128,
                                                 cpu=not args.no_cpu_baseline)

@@ -291,6 +291,13 @@ int modlin_autotune(char *report, size_t cap);
 /* Number of this library's kernel launches since load (for launch-count
  * claims in measurements). */
 uint64_t modlin_kernel_launches(void);
+/* The roofline of the plain trailing update (MODLIN_RANK_PLAIN) for modulus
+ * p: its inner loop alone (u64 x u64 -> u128 products, lazy accumulation,
+ * one reduction per safe_batch products, operands from shared memory, no
+ * global traffic) on every SM at the kernel's occupancy, in modular
+ * multiply-adds per second (best of three timed launches). No reference
+ * counterpart: it is the denominator of the plain kernel's pipe fraction. */
+int modlin_plain_mac_peak(uint64_t p, double *modmac_per_s);
 /* Failure-detection test hook (no reference counterpart; the reference has
  * no device waits): the next MODLIN_LC_GRID launch in this process bounds
  * each grid-barrier wait by spin_cycles (1 .. 4e9) instead of ~1 s, and its

@@ -210,9 +210,9 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   if (tc) {
     CK(C->tcA.ensure(tc_a_bytes(n)));
     CK(C->tcB.ensure(tc_b_bytes(n)));
-    CK(C->tcerr.ensure(2 * sizeof(int)));
-    CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
   }
+  CK(C->tcerr.ensure(2 * sizeof(int)));
+  CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
   uint64_t* Lbuf = C->lbuf.as<uint64_t>();
   uint64_t* Ubuf = C->ubuf.as<uint64_t>();
   uint64_t* Upanel = C->upanel.as<uint64_t>();
@@ -510,7 +510,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
                               C->tcB.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
         g_launches += 3;
       } else {
-        launch_trailing_plain<F>(f, R.m, ld, r0 + pb, n, jend, n, Lbuf, r0, Ubuf, n, pb, st);
+        launch_trailing_plain<F>(f, R.m, ld, r0 + pb, n, jend, n, Lbuf, r0, Ubuf, n, pb, C->tcerr.as<int>(), st);
         g_launches++;
       }
       cudaEventRecord(evp.second, st);
@@ -525,7 +525,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
   }
   CK(cudaStreamSynchronize(st));
-  if (tc) {
+  {
     int err = 0;
     CK(cudaMemcpy(&err, C->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return MODLIN_ETIMEOUT;
@@ -1106,14 +1106,20 @@ int modlin_trailing_update_device(uint64_t p, uint64_t* d_C, size_t ldc, size_t 
   std::lock_guard<std::mutex> g(C->mu);
   cudaStream_t st = user_stream(stream);
   if (kernel == MODLIN_RANK_PLAIN) {
+    CK(C->tcerr.ensure(2 * sizeof(int)));
+    CK(cudaMemsetAsync(C->tcerr.p, 0, 2 * sizeof(int), st));
     if (p == kM61)
       launch_trailing_plain<FpM61>(FpM61(fp), d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U, (int64_t)ldu,
-                                   (int)K, st);
+                                   (int)K, C->tcerr.as<int>(), st);
     else
       launch_trailing_plain<FpBarrett>(FpBarrett(fp), d_C, (int64_t)ldc, 0, (int)M, 0, (int)N, d_L, 0, d_U,
-                                       (int64_t)ldu, (int)K, st);
+                                       (int64_t)ldu, (int)K, C->tcerr.as<int>(), st);
     g_launches++;
     CK(cudaGetLastError());
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, C->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return MODLIN_ETIMEOUT;
   } else {
     CK(C->tcA.ensure(tc_a_bytes((int)M)));
     CK(C->tcB.ensure(tc_b_bytes((int)N)));
@@ -1569,6 +1575,49 @@ int modlin_testing_grid_timeout_once(long long spin_cycles, int skip_cta) {
 double modlin_last_trailing_ms(void) { return g_last_trailing_ms; }
 
 double modlin_last_trailing_macs(void) { return g_last_trailing_macs; }
+
+int modlin_plain_mac_peak(uint64_t p, double* modmac_per_s) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!modmac_per_s) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  const bool m61 = p == kM61;
+  const int per_sm = m61 ? plain_blocks_per_sm<FpM61>() : plain_blocks_per_sm<FpBarrett>();
+  const int blocks = C->num_sms * (per_sm > 0 ? per_sm : 1);
+  const int iters = 64;
+  CK(C->bmout.ensure((size_t)blocks * 256 * 8));
+  cudaStream_t st = C->stream;
+  auto launch = [&]() {
+    return m61 ? launch_plain_mac_peak(FpM61(fp), blocks, iters, C->bmout.as<uint64_t>(), st)
+               : launch_plain_mac_peak(FpBarrett(fp), blocks, iters, C->bmout.as<uint64_t>(), st);
+  };
+  CK(launch());  // warm-up
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int r = 0; r < 3; ++r) {
+    cudaEventRecord(e0, st);
+    const cudaError_t e = launch();
+    cudaEventRecord(e1, st);
+    if (e != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return MODLIN_ECUDA;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g_launches += 4;
+  *modmac_per_s = (double)blocks * 256 * 16 * 64 * iters / (best * 1e-3);
+  return MODLIN_OK;
+}
 
 // ---- Batch plans: device state built once, launches that can be captured.
 }  // extern "C"

@@ -5,6 +5,7 @@
 
 #include "rank_plain.cuh"
 #include "rank_kernels.cuh"
+#include "tc_ptx.cuh"
 
 namespace modlin {
 
@@ -248,22 +249,65 @@ __global__ void clear_pivot_flags_kernel(const PanelState* ps, uint8_t* is_pivot
 }
 
 // ---------------------------------------------------------------------------
-// trailing_plain_kernel — A[rbeg.., jend..] -= L * U mod p on the integer
+// trailing_plain_kernel — A[rbeg.., jend..cend) -= L * U mod p on the integer
 // pipes (src/fp.rs:208-248): 64x64 output tile per CTA, 4x4 per thread,
-// u128 accumulators, one reduction per safe_batch products.
+// u128 accumulators, one reduction per safe_batch products. The operands of
+// the whole depth K are staged in shared memory by bulk copies
+// (cp.async.bulk, completion counted on one mbarrier) that warp 0 issues:
+// the tile's 64 rows of L (row stride 64, so one contiguous block) and K rows
+// of 64 columns of U (one 512-byte copy each). U rows that are not 16-byte
+// aligned or run past cend, and an unaligned L, are loaded by the threads.
+// The mbarrier wait is bounded; on expiry the CTA records err[0] = 1, waits
+// (bounded) for its own copies and returns without writing C.
 // ---------------------------------------------------------------------------
+constexpr int kPlainSmem = 2 * 64 * 64 * 8;  // L tile + U tile
+
 template <class F>
 __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __restrict__ m, int64_t ld, int32_t rbeg,
                                                               int32_t n, int32_t jend, int32_t cend,
                                                               const uint64_t* __restrict__ Lbuf, int32_t r0,
                                                               const uint64_t* __restrict__ Ubuf, int64_t ldU,
-                                                              int32_t K) {
-  constexpr int KC = 32;  // K chunk staged in shared memory
-  __shared__ uint64_t Ls[KC][64 + 1];
-  __shared__ uint64_t Us[KC][64];
+                                                              int32_t K, int* err) {
+  extern __shared__ __align__(128) uint64_t smem_plain[];
+  uint64_t* Ls = smem_plain;            // [64][64]: tile row ri, depth k
+  uint64_t* Us = smem_plain + 64 * 64;  // [64][64]: depth k, tile column ci
+  __shared__ __align__(8) uint64_t bar;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int64_t rt = (int64_t)rbeg + (int64_t)blockIdx.y * 64;
   const int64_t ct = (int64_t)jend + (int64_t)blockIdx.x * 64;
+  const int rows = n - rt < 64 ? (int)(n - rt) : 64;
+  const uint64_t* lsrc = Lbuf + (rt - r0) * kPanel;
+  const bool bulk_l = ((uintptr_t)lsrc & 15) == 0;
+  const bool bulk_u = ct + 64 <= cend && ((uintptr_t)(Ubuf + ct) & 15) == 0 && (ldU & 1) == 0;
+  const uint32_t bytes = (bulk_l ? (uint32_t)rows * 512u : 0u) + (bulk_u ? (uint32_t)K * 512u : 0u);
+  if (tid == 0) {
+    tc::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid < 32 && bytes) {
+    if (tid == 0) tc::mbar_arrive_expect_tx(&bar, bytes);
+    __syncwarp();
+    if (bulk_l && tid == 0) tc::bulk_g2s(Ls, lsrc, (uint32_t)rows * 512u, &bar);
+    if (bulk_u)
+      for (int k = tid; k < K; k += 32) tc::bulk_g2s(Us + k * 64, Ubuf + (int64_t)k * ldU + ct, 512u, &bar);
+  }
+  if (!bulk_l)
+    for (int idx = tid; idx < rows * 64; idx += 256) Ls[idx] = lsrc[(idx >> 6) * kPanel + (idx & 63)];
+  if (!bulk_u)
+    for (int idx = tid; idx < K * 64; idx += 256) {
+      const int k = idx >> 6, ci = idx & 63;
+      Us[idx] = ct + ci < cend ? Ubuf[(int64_t)k * ldU + ct + ci] : 0;
+    }
+  bool ok = true;
+  if (bytes) ok = tc::mbar_wait(&bar, 0, err);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      if (bytes) tc::mbar_wait(&bar, 0, err + 1);  // this CTA's copies land before it exits
+    }
+    return;
+  }
   const uint64_t sb = f.safe_batch();
   uint64_t tot[4][4];
   u128 acc[4][4];
@@ -275,25 +319,79 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
       acc[i][q] = 0;
     }
   uint64_t cnt = 0;
-  for (int k0 = 0; k0 < K; k0 += KC) {
-    const int kc = min(KC, K - k0);
-    for (int idx = tid; idx < 64 * kc; idx += 256) {
-      const int ri = idx / kc, k = idx - ri * kc;
-      const int64_t r = rt + ri;
-      Ls[k][ri] = r < n ? Lbuf[(r - r0) * kPanel + k0 + k] : 0;
+  for (int k = 0; k < K; ++k) {
+    uint64_t a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = Ls[(ty + 16 * i) * 64 + k];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) b[q] = Us[k * 64 + tx + 16 * q];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][q] += (u128)a[i] * b[q];
+    if (++cnt == sb) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          tot[i][q] = f.add(tot[i][q], f.reduce(acc[i][q]));
+          acc[i][q] = 0;
+        }
+      cnt = 0;
     }
-    for (int idx = tid; idx < 64 * kc; idx += 256) {
-      const int k = idx >> 6, ci = idx & 63;
-      const int64_t c = ct + ci;
-      Us[k][ci] = c < cend ? Ubuf[(int64_t)(k0 + k) * ldU + c] : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t r = rt + ty + 16 * i;
+    if (r >= n) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t c = ct + tx + 16 * q;
+      if (c < cend) {
+        uint64_t* p = m + r * ld + c;
+        *p = f.sub(*p, f.add(tot[i][q], f.reduce(acc[i][q])));
+      }
     }
-    __syncthreads();
-    for (int k = 0; k < kc; ++k) {
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plain_mac_peak_kernel — the roofline of trailing_plain_kernel: its inner
+// loop (4x4 u128 accumulators per thread, operands read from shared memory,
+// one reduction per safe_batch products) run `iters` times over a 64-deep
+// tile that stays in shared memory, with no global traffic. The sums are
+// written out so that nothing is optimised away.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) plain_mac_peak_kernel(F f, int iters, uint64_t* out) {
+  extern __shared__ __align__(128) uint64_t smem_peak[];
+  uint64_t* Ls = smem_peak;
+  uint64_t* Us = smem_peak + 64 * 64;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const uint64_t p = f.modulus();
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    Ls[idx] = (0x9E3779B97F4A7C15ull * (uint64_t)(idx + 1 + blockIdx.x)) % p;
+    Us[idx] = (0xBF58476D1CE4E5B9ull * (uint64_t)(idx + 7)) % p;
+  }
+  __syncthreads();
+  const uint64_t sb = f.safe_batch();
+  uint64_t tot[4][4];
+  u128 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      tot[i][q] = 0;
+      acc[i][q] = 0;
+    }
+  uint64_t cnt = 0;
+  for (int it = 0; it < iters; ++it)
+    for (int k = 0; k < 64; ++k) {
       uint64_t a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = Ls[k][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = Ls[(ty + 16 * i) * 64 + k];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) b[q] = Us[k][tx + 16 * q];
+      for (int q = 0; q < 4; ++q) b[q] = Us[k * 64 + tx + 16 * q];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -309,21 +407,29 @@ __global__ void __launch_bounds__(256) trailing_plain_kernel(F f, uint64_t* __re
         cnt = 0;
       }
     }
-    __syncthreads();
-  }
+  uint64_t s = 0;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int64_t r = rt + ty + 16 * i;
-    if (r >= n) continue;
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int64_t c = ct + tx + 16 * q;
-      if (c < cend) {
-        uint64_t* p = m + r * ld + c;
-        *p = f.sub(*p, f.add(tot[i][q], f.reduce(acc[i][q])));
-      }
-    }
-  }
+    for (int q = 0; q < 4; ++q) s ^= f.add(tot[i][q], f.reduce(acc[i][q]));
+  out[(int64_t)blockIdx.x * 256 + tid] = s;
+}
+
+template <class F>
+cudaError_t launch_plain_mac_peak(const F& f, int blocks, int iters, uint64_t* out, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(plain_mac_peak_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kPlainSmem);
+  if (e != cudaSuccess) return e;
+  plain_mac_peak_kernel<F><<<blocks, 256, kPlainSmem, st>>>(f, iters, out);
+  return cudaGetLastError();
+}
+
+template <class F>
+int plain_blocks_per_sm() {
+  cudaFuncSetAttribute(trailing_plain_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlainSmem);
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, trailing_plain_kernel<F>, 256, kPlainSmem);
+  return nb;
 }
 
 // ---------------------------------------------------------------------------
@@ -739,10 +845,17 @@ void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st
 
 template <class F>
 void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
-                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st) {
+                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, int* err,
+                           cudaStream_t st) {
   if (rbeg >= rend || jend >= cend || K <= 0) return;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trailing_plain_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlainSmem);
+    attr = true;
+  }
   dim3 grid((cend - jend + 63) / 64, (rend - rbeg + 63) / 64);
-  trailing_plain_kernel<F><<<grid, 256, 0, st>>>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K);
+  trailing_plain_kernel<F><<<grid, 256, kPlainSmem, st>>>(f, m, ld, rbeg, rend, jend, cend, Lbuf, r0, Ubuf, ldU, K,
+                                                           err);
 }
 
 template <class F>
@@ -777,7 +890,9 @@ void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint6
   template void launch_couple<F>(const F&, const uint64_t*, int64_t, int, int, const PanelState*,               \
                                  const uint64_t*, uint64_t*, int64_t, cudaStream_t);                            \
   template void launch_trailing_plain<F>(const F&, uint64_t*, int64_t, int, int, int, int, const uint64_t*, int, \
-                                         const uint64_t*, int64_t, int, cudaStream_t);
+                                         const uint64_t*, int64_t, int, int*, cudaStream_t);                        \
+  template cudaError_t launch_plain_mac_peak<F>(const F&, int, int, uint64_t*, cudaStream_t);                      \
+  template int plain_blocks_per_sm<F>();
 
 INSTANTIATE(FpBarrett)
 INSTANTIATE(FpM61)

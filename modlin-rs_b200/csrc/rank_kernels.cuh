@@ -31,8 +31,18 @@ void launch_couple(const F& f, const uint64_t* m, int64_t ld, int n, int jend, c
 void launch_moves(uint64_t* m, int64_t ld, int n, int jend, const int2* moves, int nmoves, uint64_t* Lbuf, int r0,
                   int pb, cudaStream_t st);
 void launch_clear_flags(const PanelState* ps, uint8_t* is_pivot, cudaStream_t st);
+// err: device error words (err[0] = 1 when a bounded wait expired).
 template <class F>
 void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
-                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, cudaStream_t st);
+                           const uint64_t* Lbuf, int r0, const uint64_t* Ubuf, int64_t ldU, int K, int* err,
+                           cudaStream_t st);
+// The plain trailing update's arithmetic alone (its inner loop on operands
+// resident in shared memory, `iters` passes of depth 64 per thread): blocks x
+// 256 x 16 x 64 x iters modular multiply-adds. The CTAs per SM that
+// trailing_plain_kernel reaches are given by plain_blocks_per_sm.
+template <class F>
+cudaError_t launch_plain_mac_peak(const F& f, int blocks, int iters, uint64_t* out, cudaStream_t st);
+template <class F>
+int plain_blocks_per_sm();
 
 }  // namespace modlin

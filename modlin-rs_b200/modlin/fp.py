@@ -221,3 +221,12 @@ class BatchPlan:
             self.free()
         except Exception:
             pass
+
+
+def plain_mac_peak(field) -> float:
+    """Modular multiply-adds per second of the plain trailing update's inner
+    loop alone (shared-memory operands, no global traffic): the plain
+    kernel's roofline on this GPU."""
+    out = ctypes.c_double(0)
+    check(lib().modlin_plain_mac_peak(_p(field), ctypes.byref(out)), "plain_mac_peak")
+    return out.value
