@@ -790,7 +790,7 @@ def main():
     from modlin import fp as mfp
 
     # The AUTO choices measured on this GPU (a few seconds, before any timing).
-    tune = modlin.autotune()["choice"] if not args.no_autotune else None
+    tune = modlin.autotune()["choice"] if not args.no_autotune and args.workload != "trailing" else None
 
     if args.workload == "bm":
         res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup)

@@ -2,6 +2,8 @@
 // the linear-complexity drivers, batches and the workload generators.
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -789,6 +791,10 @@ static int crossover(const std::vector<int>& sizes, const std::vector<bool>& fas
     }                                                                                   \
   } while (0)
 
+// Timings in the tuner's JSON report: a non-finite value (a failed or
+// unmeasurable timing) is written as -1 so that the report stays valid JSON.
+static double finite_ms(double t) { return std::isfinite(t) ? t : -1.0; }
+
 static int autotune_locked(Ctx* C, std::string& rep) {
   int rc = MODLIN_OK;
   cudaStream_t st = C->stream;
@@ -823,7 +829,7 @@ static int autotune_locked(Ctx* C, std::string& rep) {
       }
       tc_wins.push_back(t[1] <= t[0]);
       std::snprintf(buf, sizeof buf, "%s\"%d-limb n=%d\": [%.3f, %.3f]", rep.back() == '{' ? "" : ", ",
-                    1 << li, n, t[0], t[1]);
+                    1 << li, n, finite_ms(t[0]), finite_ms(t[1]));
       rep += buf;
     }
     T.tc_cross[li] = crossover(sizes, tc_wins, 1 << 30);
@@ -858,7 +864,7 @@ static int autotune_locked(Ctx* C, std::string& rep) {
         best = t;
         best_thr = thr[q];
       }
-      std::snprintf(buf, sizeof buf, "%s\"below %d\": %.3f", q == 0 ? "" : ", ", thr[q], t);
+      std::snprintf(buf, sizeof buf, "%s\"below %d\": %.3f", q == 0 ? "" : ", ", thr[q], finite_ms(t));
       rep += buf;
     }
     C->tune.two_panel_min = saved;
@@ -897,7 +903,8 @@ static int autotune_locked(Ctx* C, std::string& rep) {
         if (rc) return rc;
       }
       tc_wins.push_back(t[1] <= t[0]);
-      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == bsz[0] ? "" : ", ", n, t[0], t[1]);
+      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == bsz[0] ? "" : ", ", n, finite_ms(t[0]),
+                    finite_ms(t[1]));
       rep += buf;
     }
     rep += "}";
@@ -929,7 +936,7 @@ static int autotune_locked(Ctx* C, std::string& rep) {
       }, &rc);
       if (rc) return rc;
       std::snprintf(buf, sizeof buf, "%s\"n=%lld t=%d\": %.3f", rep.back() == '{' ? "" : ", ",
-                    (long long)bm_len[c], t, ms);
+                    (long long)bm_len[c], t, finite_ms(ms));
       rep += buf;
       if (ms < best) {
         best = ms;
@@ -962,7 +969,8 @@ static int autotune_locked(Ctx* C, std::string& rep) {
       }, &rc);
       if (rc) return rc;
       cl_wins.push_back(tcl <= tblk);
-      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == csz[0] ? "" : ", ", n, tblk, tcl);
+      std::snprintf(buf, sizeof buf, "%s\"n=%d\": [%.3f, %.3f]", n == csz[0] ? "" : ", ", n, finite_ms(tblk),
+                    finite_ms(tcl));
       rep += buf;
     }
     T.bm_cluster_min = crossover(csz, cl_wins, 1 << 30);
@@ -1006,7 +1014,7 @@ static int autotune_locked(Ctx* C, std::string& rep) {
             return rc;
           }
           std::snprintf(buf, sizeof buf, "%s\"max<%lld t=%d smem=%dK\": %.3f", rep.back() == '{' ? "" : ", ",
-                        (long long)hi[c], t, kib, ms);
+                        (long long)hi[c], t, kib, finite_ms(ms));
           rep += buf;
           if (ms < best) {
             best = ms;
