@@ -34,9 +34,12 @@
 // while the epilogue drains subtile s. Every
 // mbarrier wait is bounded; on expiry the kernel records an error, drains
 // its own copies and MMAs (bounded), frees TMEM and returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <climits>
+#include <cstring>
 #include <cstdint>
 #include <type_traits>
 
@@ -72,10 +75,10 @@ struct Shape {
   static constexpr int C_BYTES = LIMBS == 8 ? CDEPTH * 128 * kCStride * 8 : 0;  // staged C tiles
   static constexpr int SMEM = A_BYTES + STAGES * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
   static_assert(SMEM <= 227 * 1024, "shared memory");
-  // p = 2^61 - 1: the epilogue keeps C in registers, so the shared memory of
-  // the staged C tiles goes to a deeper B ring.
-  static constexpr int STAGES_M61 = KK == 64 ? 8 : 5;
-  static constexpr int SMEM_M61 = A_BYTES + STAGES_M61 * B_BYTES + ZERO_BYTES + 1024;
+  // p = 2^61 - 1: the epilogue stages C by TMA, one 128 x 16 tile per group.
+  static constexpr int STAGES_M61 = KK == 64 ? 8 : 3;
+  static constexpr int C_TMA_BYTES = 2 * 128 * 16 * 8;  // one 128 x 16 C tile per epilogue group
+  static constexpr int SMEM_M61 = A_BYTES + STAGES_M61 * B_BYTES + ZERO_BYTES + 1024 + C_TMA_BYTES;
   static_assert(SMEM_M61 <= 227 * 1024, "shared memory");
 };
 
@@ -196,7 +199,8 @@ __device__ __forceinline__ uint64_t m61_sub_lazy(uint64_t cv, uint64_t x) {
 template <class F, int LIMBS, int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
-                       int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err) {
+                       int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err,
+                       const __grid_constant__ CUtensorMap cmap, int use_tma) {
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
   // p = 2^61 - 1: two epilogue groups of 8 warps, one per accumulator buffer.
@@ -229,6 +233,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(acc_empty + b, kM61Path ? kEpiWarps / 2 : kEpiWarps);
     }
     mbar_init(mma_done, 1);
+    mbar_init(bars + 40, 1);  // c_full of epilogue group 0 (p = 2^61 - 1 with TMA)
+    mbar_init(bars + 41, 1);  // c_full of epilogue group 1
     for (int st = 0; st < kStages; ++st) {
       mbar_init(b_full + st, 1);
       mbar_init(b_empty + st, 1);
@@ -324,18 +330,25 @@ __global__ void __launch_bounds__(kThreads, 1)
     // subtiles it = g, g + 2, ... of this CTA's range, so each group has two
     // MMA periods per subtile and the groups' phases interleave. In a group,
     // warp w reads TMEM lanes 32*(w%4)..+32 (its 32 rows) and one half (8
-    // columns) of the 16-column subtile; every thread owns one row x 8
-    // columns: it loads their C values from global memory one subtile ahead
-    // (into registers), folds the 15 diagonal sums of each column, releases
-    // the buffer, and stores C - T. No shared memory, no barriers between
-    // warps.
+    // columns) of the 16-column subtile, so every thread owns one row x 8
+    // columns. It folds the 15 diagonal sums of each column and releases the
+    // accumulator buffer first; then C - T is formed against C.
+    // C moves by TMA (use_tma): the group's leader thread loads the 128 x 16
+    // C tile of its next subtile into the group's shared buffer (128-byte
+    // swizzle, so the threads' row-wise accesses are conflict-free), the
+    // threads replace it in place by C - T, and the leader stores it back
+    // with one tensor copy, then loads the group's next tile. Without TMA
+    // (a row stride or column offset that is not 16-byte aligned) every
+    // thread reads and writes its 8 values directly.
     const int ew = warp - 2;
     const int grp = ew >> 3;          // accumulator buffer this group drains
     const int quad = warp & 3;        // TMEM lane quadrant
     const int half = (ew >> 2) & 1;   // column half of the subtile
     const int row = quad * 32 + lane;
+    const bool leader = (ew & 7) == 0 && lane == 0;
     const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + grp * 256 + half * 8;
-    const bool vec = (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0;
+    uint64_t* cbuf = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024) + grp * (128 * 16);
+    uint64_t* c_full = bars + 40 + grp;
     const int64_t nsub = S.nsub;
     // Subtile it = grp + 2 k of [g0, g1): (mt, sb) tracked incrementally.
     int64_t g = g0 + grp;
@@ -348,60 +361,96 @@ __global__ void __launch_bounds__(kThreads, 1)
         ++mt;
       }
     };
+    int loads = 0;  // TMA loads issued by the leader (c_full phases)
+    auto tma_load = [&]() {
+      mbar_arrive_expect_tx(c_full, 128 * 16 * 8);
+      tma_load_2d(cbuf, &cmap, (int32_t)(jend + sb * NS), (int32_t)(rbeg + mt * 128), c_full);
+      ++loads;
+    };
     auto load_c = [&](uint64_t (&cv)[8]) {
       const int64_t r = (int64_t)rbeg + mt * 128 + row;
       const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
       const uint64_t* src = m + r * ld + c0;
-      if (r < rend && vec && c0 + 8 <= cend) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2*>(src) + q);
-          cv[2 * q] = v.x;
-          cv[2 * q + 1] = v.y;
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) cv[c] = (r < rend && c0 + c < cend) ? __ldcs(src + c) : 0;
-      }
+      for (int c = 0; c < 8; ++c) cv[c] = (r < rend && c0 + c < cend) ? __ldcs(src + c) : 0;
     };
     uint64_t cv[8];
-    if (g < g1) load_c(cv);
+    if (g < g1) {
+      if (!use_tma)
+        load_c(cv);
+      else if (leader)
+        tma_load();
+    }
     bool ok = true;
     for (int k = 0; g < g1; ++k) {
-      if (!(ok = __all_sync(0xffffffffu, mbar_wait(acc_full + grp, k & 1, err)))) break;
-      fence_after();
+      bool okw = __all_sync(0xffffffffu, mbar_wait(acc_full + grp, k & 1, err));
       uint64_t x[8];
+      if (okw) {
+        fence_after();
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        uint32_t a[15][4];
+        for (int q = 0; q < 2; ++q) {
+          uint32_t a[15][4];
 #pragma unroll
-        for (int d = 0; d < 15; ++d) tmem_ld4(lane_base + d * NS + q * 4, a[d]);
-        tmem_wait_ld();
+          for (int d = 0; d < 15; ++d) tmem_ld4(lane_base + d * NS + q * 4, a[d]);
+          tmem_wait_ld();
 #pragma unroll
-        for (int c = 0; c < 4; ++c) x[4 * q + c] = m61_fold15(a, c);
+          for (int c = 0; c < 4; ++c) x[4 * q + c] = m61_fold15(a, c);
+        }
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty + grp);
       }
-      fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty + grp);
-      const int64_t r = (int64_t)rbeg + mt * 128 + row;
-      const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
-      uint64_t res[8];
+      if (use_tma) {
+        if (okw) okw = __all_sync(0xffffffffu, mbar_wait(c_full, k & 1, err));
+        if (okw) {
+          // Row `row`, 16-byte chunks 4 half .. +4 of the 128-byte row; the
+          // 128-byte swizzle XORs the chunk index (address bits 4-6) with
+          // address bits 7-9.
+          uint64_t* rp = cbuf + row * 16;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) res[c] = m61_sub_lazy(cv[c], x[c]);
-      uint64_t* dst = m + r * ld + c0;
-      if (r < rend) {
-        if (vec && c0 + 8 <= cend) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            __stcs(reinterpret_cast<ulonglong2*>(dst) + q, make_ulonglong2(res[2 * q], res[2 * q + 1]));
-        } else {
+          for (int q = 0; q < 4; ++q) {
+            uint64_t* lp = rp + (half * 4 + q) * 2;
+            const uint32_t a = smem_u32(lp);
+            const int delta = (int)((a ^ (a >> 3)) & 0x70u) - (int)(a & 0x70u);
+            ulonglong2* pq = reinterpret_cast<ulonglong2*>(reinterpret_cast<uint8_t*>(lp) + delta);
+            const ulonglong2 v = *pq;
+            *pq = make_ulonglong2(m61_sub_lazy(v.x, x[2 * q]), m61_sub_lazy(v.y, x[2 * q + 1]));
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        // Every thread of the group reaches this barrier, failed or not; the
+        // group leaves together when any of them failed.
+        if (!group_bar_and(1 + grp, okw)) {
+          ok = false;
+          break;
+        }
+        if (leader) {
+          tma_store_2d(&cmap, (int32_t)(jend + sb * NS), (int32_t)(rbeg + mt * 128), cbuf);
+          bulk_commit();
+          bulk_wait_read0();  // the buffer is read; it can take the next tile
+        }
+        advance();
+        if (leader && g < g1) tma_load();
+      } else {
+        if (!okw) {
+          ok = false;
+          break;
+        }
+        const int64_t r = (int64_t)rbeg + mt * 128 + row;
+        const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
+        uint64_t* dst = m + r * ld + c0;
+        if (r < rend) {
 #pragma unroll
           for (int c = 0; c < 8; ++c)
-            if (c0 + c < cend) dst[c] = res[c];
+            if (c0 + c < cend) dst[c] = m61_sub_lazy(cv[c], x[c]);
         }
+        advance();
+        if (g < g1) load_c(cv);
       }
-      advance();
-      if (g < g1) load_c(cv);
+    }
+    if (leader && use_tma) {
+      bulk_wait_all0();  // stores complete
+      if (!ok && loads > 0) mbar_wait(c_full, (loads - 1) & 1, err + 1);  // a load still landing
     }
     if (!ok) atomicExch(err, 1);
   } else {
@@ -627,6 +676,30 @@ void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_
   split_b_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(B, ldb, jend, cend, K, npad, Bw);
 }
 
+// Tensor map of C = m[0 .. rend) x [0 .. cend) (row stride ld) for 128 x 16
+// boxes of u64 with the 128-byte swizzle; false when the driver entry point
+// is unavailable or the encoding fails.
+static bool make_c_map(CUtensorMap* map, uint64_t* m, int64_t ld, int rend, int cend) {
+  static PFN_cuTensorMapEncodeTiled encode = []() -> PFN_cuTensorMapEncodeTiled {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  }();
+  if (!encode) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cend, (cuuint64_t)rend};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+  const cuuint32_t box[2] = {16, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, m, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class F, int LIMBS, int KK>
 void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint8_t* Aw,
               const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st) {
@@ -642,8 +715,14 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
     cudaFuncSetAttribute(trailing_tc_kernel<F, LIMBS, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
+  // C through TMA (p = 2^61 - 1): 16-byte aligned rows and column offset.
+  CUtensorMap cmap;
+  std::memset(&cmap, 0, sizeof cmap);
+  int use_tma = 0;
+  if (std::is_same<F, FpM61>::value && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0)
+    use_tma = make_c_map(&cmap, m, ld, rend, cend) ? 1 : 0;
   trailing_tc_kernel<F, LIMBS, KK><<<grid, kThreads, smem, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64,
-                                                                  err);
+                                                                  err, cmap, use_tma);
 }
 
 // (limb count, K tile) of a prime and an update depth.
