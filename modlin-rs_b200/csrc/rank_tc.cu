@@ -1,8 +1,8 @@
 // Exact modular trailing update on the 5th-generation tensor cores.
 //
-//   C[rbeg.., jend..] -= L * U  (mod p),   L: M x K,  U: K x N,  K = pb <= 64,
+//   C[rbeg.., jend..] -= L * U  (mod p),   L: M x K,  U: K x N,  K <= 128,
 //
-// the rank-pb update of the reference's blocked elimination
+// the rank-K update of the reference's blocked elimination
 // (src/fp.rs:202-248), recast as integer GEMMs that are exact:
 //
 // * Every residue x < p is split into LIMBS unsigned 8-bit limbs,
@@ -14,26 +14,31 @@
 //   writes TMEM columns [i*NS, i*NS + 128), so the product L_i U_j lands in
 //   column block i+j: the diagonal sums S_d accumulate in TMEM for free.
 //   2*LIMBS-1 blocks of NS columns (240 of the 256 allocated for LIMBS = 8).
-// * No overflow: S_d <= LIMBS * K * 255^2 < 2^26 for K <= 64.
+//   Plane 0 initialises blocks 0..LIMBS-1 and the first K step of plane
+//   LIMBS-1 is split in two MMAs so that it initialises the upper blocks.
+// * No overflow: S_d <= LIMBS * K * 255^2 < 2^27 for K <= 128.
 // * Epilogue: T = sum_d 2^(8d) S_d reduced exactly mod p (for 2^61 - 1 the
-//   weights are powers of two mod p, so pairs of blocks fold into 32-bit
-//   words), then C = C - T mod p. Bit-exact against the u64 Barrett path.
+//   weights are powers of two mod p, so the 15 blocks fold into one value
+//   below 2^62 with 32-bit multiply-adds), then C = C - T mod p. Bit-exact
+//   against the u64 Barrett path.
 //
-// Operands are staged by cp.async.bulk (no tensor maps) in the canonical
-// K-major, no-swizzle UMMA layout: 8-row x 16-byte core matrices, LBO = 128 B
-// between the core matrices along K, SBO = 512 B between 8-row groups. The
-// limb planes are written to global memory in exactly that layout by the
-// split kernels, so each stage is one contiguous bulk copy.
+// Operands are staged by cp.async.bulk in the canonical K-major, no-swizzle
+// UMMA layout: 8-row x 16-byte core matrices, LBO = 128 B between the core
+// matrices along K, SBO = 8 K B between 8-row groups. The limb planes are
+// written to global memory in exactly that layout by the split kernels, so
+// each stage is one contiguous bulk copy.
 //
 // CTA = 18 warps: warp 0 issues the bulk copies, warp 1 owns TMEM and issues
-// the MMAs (one thread), warps 2-17 drain TMEM (warp w reads lanes
-// 32*(w%4)..+32, 4 of every 16 columns). Each CTA takes a contiguous range of
-// the (M tile, N subtile) space; it keeps the 128-row A tile (all limb planes) resident
-// and streams B subtiles through a 6-stage ring; one CTA per SM owns all 512
-// TMEM columns as two accumulator buffers, so the MMAs of subtile s+1 run
-// while the epilogue drains subtile s. Every
-// mbarrier wait is bounded; on expiry the kernel records an error, drains
-// its own copies and MMAs (bounded), frees TMEM and returns.
+// the MMAs (one thread), warps 2-17 drain TMEM. Each CTA takes a contiguous
+// range of the (M tile, N subtile) space; it keeps the 128-row A tile (all
+// limb planes) resident and streams B subtiles through a ring; one CTA per SM
+// owns all 512 TMEM columns as two accumulator buffers, so the MMAs of
+// subtile s+1 run while the epilogue drains subtile s. Over 2^61 - 1 the
+// epilogue is two 8-warp groups, one per accumulator buffer, and C moves by
+// 2D TMA (128 x 16 tiles, 128-byte swizzle) through one shared buffer per
+// group; other primes use 16 warps and C staged by cp.async. Every mbarrier
+// wait is bounded; on expiry the kernel records an error, drains its own
+// copies and MMAs (bounded), frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -71,7 +76,7 @@ struct Shape {
   static constexpr int CDEPTH = KK == 64 ? 4 : 2;    // staged C tiles (subtiles) in shared memory
   static constexpr int A_BYTES = LIMBS * TILE;       // resident A tile
   static constexpr int B_BYTES = TILE;               // one B subtile (all planes)
-  static constexpr int ZERO_BYTES = 4096;            // zero A tile (128 x 32 B)
+  static constexpr int ZERO_BYTES = 0;
   static constexpr int C_BYTES = LIMBS == 8 ? CDEPTH * 128 * kCStride * 8 : 0;  // staged C tiles
   static constexpr int SMEM = A_BYTES + STAGES * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
   static_assert(SMEM <= 227 * 1024, "shared memory");
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sA = smem;                        // A_BYTES
   uint8_t* sB = smem + SH::A_BYTES;          // kStages * 8 KB
-  uint8_t* sZ = sB + kStages * SH::B_BYTES;  // 4 KB of zeros
+  uint8_t* sZ = sB + kStages * SH::B_BYTES;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES);
   uint64_t* sC = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024);  // [kCDepth][128][kCStride]
   uint64_t* a_full = bars + 0;
@@ -223,8 +228,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ uint32_t tmem_base_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < SH::ZERO_BYTES / 16; i += blockDim.x)
-    reinterpret_cast<uint4*>(sZ)[i] = make_uint4(0, 0, 0, 0);
   if (threadIdx.x == 0) {
     mbar_init(a_full, 1);
     mbar_init(a_empty, 1);
@@ -247,8 +250,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // Make the zero tile visible to the tensor core (async proxy).
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   fence_before();
   __syncthreads();
   fence_after();
@@ -291,7 +292,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       int cur = -1, nload = 0, it = 0;
       bool ok = true;
       const uint32_t id_full = idesc_i8(LIMBS * NS);
-      const uint32_t id_zero = idesc_i8(LIMBS > 1 ? (LIMBS - 1) * NS : 16);
+      const uint32_t id_upper = idesc_i8(LIMBS > 1 ? (LIMBS - 1) * NS : 16);  // B planes 1 .. LIMBS-1
+      const uint32_t id_plane = idesc_i8(NS);                                  // B plane 0
       int mt = (int)(g0 / S.nsub), sb = (int)(g0 - (int64_t)mt * S.nsub);
       for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
         if (mt != cur) {
@@ -308,14 +310,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         fence_after();
         const uint8_t* bt = sB + st * SH::B_BYTES;
         const uint32_t dacc = tmem + ab * 256;
-        if (LIMBS > 1)  // zero the upper diagonal blocks: (zero A) x B, no accumulate
-          mma_i8(dacc + LIMBS * NS, smem_desc(sZ, 256), smem_desc(bt, SH::SBO), id_zero, 0);
+        // Plane 0 (first K step without accumulate) initialises diagonal
+        // blocks 0 .. LIMBS-1. The first K step of plane LIMBS-1 is split so
+        // that it initialises blocks LIMBS .. 2 LIMBS-2 (B planes 1 .. LIMBS-1,
+        // no accumulate) and adds into block LIMBS-1 (B plane 0); every other
+        // MMA accumulates.
+        auto adesc = [&](int i, int ks) { return smem_desc(sA + i * SH::TILE + ks * 256, SH::SBO); };
 #pragma unroll
-        for (int i = 0; i < LIMBS; ++i)
+        for (int ks = 0; ks < KK / 32; ++ks)
+          mma_i8(dacc, adesc(0, ks), smem_desc(bt + ks * 256, SH::SBO), id_full, ks > 0 ? 1u : 0u);
+        if (LIMBS > 1) {
+          mma_i8(dacc + LIMBS * NS, adesc(LIMBS - 1, 0), smem_desc(bt + NS * KK, SH::SBO), id_upper, 0);
+          mma_i8(dacc + (LIMBS - 1) * NS, adesc(LIMBS - 1, 0), smem_desc(bt, SH::SBO), id_plane, 1);
+#pragma unroll
+          for (int ks = 1; ks < KK / 32; ++ks)
+            mma_i8(dacc + (LIMBS - 1) * NS, adesc(LIMBS - 1, ks), smem_desc(bt + ks * 256, SH::SBO), id_full, 1);
+        }
+#pragma unroll
+        for (int i = 1; i < LIMBS - 1; ++i)
 #pragma unroll
           for (int ks = 0; ks < KK / 32; ++ks)
-            mma_i8(dacc + i * NS, smem_desc(sA + i * SH::TILE + ks * 256, SH::SBO), smem_desc(bt + ks * 256, SH::SBO),
-                   id_full, (i > 0 || ks > 0) ? 1u : 0u);
+            mma_i8(dacc + i * NS, adesc(i, ks), smem_desc(bt + ks * 256, SH::SBO), id_full, 1);
         mma_commit(b_empty + st);
         mma_commit(acc_full + ab);
       }
