@@ -249,18 +249,20 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   // Two-panel steps (128 columns, K = 128 trailing update): blocks V11 = P11^-1
   // (negated), Y = P21 V11, S = P22 - Y P12 and VS = S^-1 (negated), and the
   // look-ahead result for the next two-panel step.
-  uint64_t *V11n = nullptr, *Yb = nullptr, *Sb = nullptr, *VSn = nullptr;
+  uint64_t *V11n = nullptr, *Yb = nullptr, *Sb = nullptr, *VSn = nullptr, *Zb = nullptr, *Pn = nullptr;
   int pre128 = -1;
   uint64_t* Hb = Lbuf;  // two-panel multipliers [H1 H2], row stride 128
   const size_t blk = (size_t)kPanel * kPanel;
   if (tc) {
-    CK(C->binv.ensure(256 + 5 * blk * 8));
+    CK(C->binv.ensure(256 + 10 * blk * 8));
     CK(C->lbuf.ensure((size_t)n * 2 * kPanel * 8));
     Lbuf = Hb = C->lbuf.as<uint64_t>();
     V11n = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256) + blk;
     Yb = V11n + blk;
     Sb = Yb + blk;
     VSn = Sb + blk;
+    Zb = VSn + blk;
+    Pn = Zb + blk;  // 128 x 128, row stride 128
     CK(C->tcBn.ensure(tc_b_bytes(kPanel)));
     binv_status = C->binv.as<int>();
     Vneg = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
@@ -284,8 +286,20 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, binv_status + slot, s);
     launch_small_gemm64<F>(f, P21, ld, V11n, kPanel, nullptr, 0, Yb, kPanel, true, s);  // Y = P21 V11
     launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s);      // S = P22 - Y P12
+    launch_small_gemm64<F>(f, V11n, kPanel, P12, ld, nullptr, 0, Zb, kPanel, true, s);  // Z = V11 P12
     launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, binv_status + slot, s);
-    g_launches += 5;
+    // -P^-1 = [[-V11 - Z S^-1 Y, Z S^-1], [S^-1 Y, -S^-1]] (row stride 128):
+    // TR = Z S^-1, BL = S^-1 Y, TL = -V11 - TR Y, BR = -S^-1.
+    uint64_t* const TL = Pn;
+    uint64_t* const TR = Pn + kPanel;
+    uint64_t* const BL = Pn + 2 * blk;
+    uint64_t* const BR = BL + kPanel;
+    launch_small_gemm64<F>(f, Zb, kPanel, VSn, kPanel, nullptr, 0, TR, 2 * kPanel, true, s);
+    launch_small_gemm64<F>(f, VSn, kPanel, Yb, kPanel, nullptr, 0, BL, 2 * kPanel, true, s);
+    launch_small_gemm64<F>(f, TR, 2 * kPanel, Yb, kPanel, V11n, kPanel, TL, 2 * kPanel, true, s);
+    e = cudaMemcpy2DAsync(BR, 2 * kPanel * 8, VSn, kPanel * 8, kPanel * 8, kPanel, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    g_launches += 9;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(h_status + slot, binv_status + slot, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -302,11 +316,10 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     if (tc && n - r0 >= R.two_panel_min && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
       // Two-panel block step: P = A[r0 .. r0+128, col .. col+128) split into
       // 64 x 64 blocks [P11 P12; P21 P22]. With V11 = P11^-1 and the Schur
-      // complement S = P22 - P21 V11 P12 invertible, the multipliers of the
-      // rows below, H = X_P P^-1 = [H1 H2], come from four n x 64 x 64
-      // products,
-      //   G1 = X1 V11,  X2' = X2 - G1 P12,  H2 = X2' S^-1,  H1 = G1 - H2 Y,
-      // (Y = P21 V11), and the trailing block takes one K = 128 update
+      // complement S = P22 - P21 V11 P12 invertible, P^-1 is assembled from
+      // 64 x 64 products on the look-ahead stream (prep128), the multipliers
+      // of the rows below come from one n x 128 x 128 product H = X_P P^-1,
+      // and the trailing block takes one K = 128 update
       // A[r0+128.., col+128..] -= H * A[r0 .. r0+128, col+128..]: half the
       // epilogue work per modMAC of two one-panel updates.
       int status = pre128;
@@ -327,20 +340,11 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
         if (rows > 0) {
           CK(cudaMemsetAsync(Hb + (size_t)2 * kPanel * 2 * kPanel, 0, (size_t)rows * 2 * kPanel * 8, st));
           const int64_t H0 = 2 * kPanel;  // H rows relative to r0, stride 128
-          const uint64_t* X1 = R.m + (int64_t)r0 * ld + col;
-          // G1 = X1 V11 into H[:, 0:64).
-          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, kPanel, X1, ld, 0, V11n, kPanel, kPanel, tA, tB,
-                                C->num_sms, terr, st));
-          // X2 -= G1 P12 (rows below the block, in place).
-          CK(launch_trailing_tc(*R.fp, R.m, ld, rb, n, col + kPanel, c2, Hb, H0, r0, R.m + (int64_t)r0 * ld, ld,
-                                kPanel, tA, tB, C->num_sms, terr, st));
-          // H2 = X2' S^-1 into H[:, 64:128).
-          CK(launch_trailing_tc(*R.fp, Hb + kPanel, H0, 2 * kPanel, n - r0, 0, kPanel, X1 + kPanel, ld, 0, VSn, kPanel,
-                                kPanel, tA, tB, C->num_sms, terr, st));
-          // H1 = G1 - H2 Y.
-          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, kPanel, Hb + kPanel, H0, 0, Yb, kPanel, kPanel,
-                                tA, tB, C->num_sms, terr, st));
-          g_launches += 13;
+          const uint64_t* X = R.m + (int64_t)r0 * ld + col;
+          // H = X P^-1 = 0 - X (-P^-1), one K = 128 product.
+          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, 2 * kPanel, X, ld, 0, Pn, 2 * kPanel,
+                                2 * kPanel, tA, tB, C->num_sms, terr, st));
+          g_launches += 4;
           if (c2 < n) {
             const uint64_t* Ub = R.m + (int64_t)r0 * ld;  // the 128 pivot rows, as they are
             auto evp = take_events();
