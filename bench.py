@@ -185,6 +185,23 @@ def int8_peak_tops(torch):
         return None
 
 
+def native_oracle():
+    """The oracle built with -march=native for this host's CPU (the
+    reference's release profile uses target-cpu=native), into a per-process
+    file; the portable build when the native one cannot be built. Returns a
+    label for the CPU-baseline description. Must run before the oracle's
+    first use in this process."""
+    import oracle
+    if oracle._lib is not None:
+        return "-O3" if oracle._SO.endswith("liboracle.so") else "-O3 -march=native"
+    try:
+        oracle.use_native(f"/tmp/modlin_oracle_native_{os.getpid()}.so")
+        return "-O3 -march=native"
+    except Exception:
+        oracle.build()
+        return "-O3 (native build failed)"
+
+
 def cpu_rank_sample(threads=0, target_s=15.0):
     """The oracle's blocked rank (the reference algorithm, OpenMP over rows)
     on a uniform matrix over 2^61-1, sized from a 1024^2 probe so that the
@@ -731,8 +748,7 @@ def cpu_model():
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    import oracle
-    oracle.build()
+    flags = native_oracle()
     cores = host_cores()
     samples = []
     for i in range(args.warmup + args.steps):
@@ -742,7 +758,7 @@ def run_reference(args, rank, world):
     v = statistics.median([s["value"] for s in samples])
     n = samples[0]["n"]
     sample = (f"rank of one uniform {n}x{n} matrix over 2^61-1 per step (W={samples[0]['work']:.4g} modMAC), "
-              f"oracle restatement of src/fp.rs:125-255 with OpenMP over {cores} threads on {cpu_model()}")
+              f"oracle restatement of src/fp.rs:125-255 ({flags}) with OpenMP over {cores} threads on {cpu_model()}")
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
@@ -777,6 +793,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+
+    oracle_flags = native_oracle() if not args.no_cpu_baseline and rank == 0 else None
 
     import numpy as np
     import torch
@@ -908,6 +926,36 @@ def main():
         extras["rank_batch"] = rank_batch_measure(torch, modlin, steps=1, warmup=1, single_sample=16)
         # The generators' device fill and the README's largest rank job.
         extras["prng_fill"] = prng_fill_measure(torch, modlin)
+        # Rooflines of the other workloads. Integer-pipe work against the
+        # measured u64 multiply-accumulate peak (the plain trailing update's
+        # inner loop alone, all SMs); tensor-core work against the int8 GEMM.
+        peak_int = extras["trailing_update"]["plain_mac_peak_modmac_per_s"]
+        int8 = int8_peak_tops(torch)
+        int_src = "measured: u64 x u64 -> u128 multiply-accumulate loop on operands in shared memory, all SMs " \
+                  "(modlin_plain_mac_peak)"
+        bm = extras["berlekamp_massey"]
+        if "mac_per_s" in bm["batch"]:
+            a = bm["batch"]["mac_per_s"]
+            bm["batch"]["roofline"] = {"bound": "latency: one block barrier per sequence step", "achieved": a,
+                                       "peak": peak_int, "unit": "modMAC/s", "frac": a / peak_int,
+                                       "peak_source": int_src}
+        for key in ("long_planted", "long_iid"):
+            e = bm[key]
+            if "mac_per_s" in e.get("cluster", {}):
+                a, pk = e["cluster"]["mac_per_s"], peak_int * 16 / 148
+                e["roofline"] = {"bound": "latency: one 16-CTA cluster barrier per step", "achieved": a, "peak": pk,
+                                 "unit": "modMAC/s", "frac": a / pk,
+                                 "peak_source": int_src + ", scaled to the cluster's 16 SMs"}
+        rb = extras["rank_batch"]
+        rb["roofline"] = {"bound": "integer pipes (panel method per CTA)", "achieved": rb["modmac_per_s"],
+                          "peak": peak_int, "unit": "modMAC/s", "frac": rb["modmac_per_s"] / peak_int,
+                          "peak_source": int_src}
+        rp = extras["rank_planted"]
+        if int8:
+            a = rp["tc"]["modmac_per_s"] * 128 / 1e12
+            rp["roofline"] = {"bound": "tensor", "achieved": a, "peak": int8, "unit": "TFLOP/s", "frac": a / int8,
+                              "peak_source": "measured: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
+                              "note": "whole planted rank: all its modMACs x 64 limb products x 2 ops / rank time"}
 
     # End to end through the public C ABI with host buffers: pinned host
     # matrix -> modlin_rank (H2D copy + rank + D2H of the result) each step.
@@ -935,7 +983,29 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = {"value": W * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": 8,
-           "ms_per_step": e2e_s * 1e3}
+           "ms_per_step": e2e_s * 1e3, "host_memory": "pinned"}
+    # The same call on pageable host memory (a Rust Vec<u64> or a numpy array
+    # is pageable): the driver stages the copy through its own pinned buffers.
+    hpage = np.array(hnp, copy=True)
+    hpp = hpage.ctypes.data_as(u64p)
+
+    def e2e_page_step():
+        rc = lib().modlin_rank_ex(M61, hpp, n, ctypes.byref(opts), ctypes.byref(out), None,
+                                  ctypes.cast(None, modlin._lib.PROGRESS), None)
+        assert rc == 0 and out.value == r
+    e2e_page_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_page_step()
+    e2e_p = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_p], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_p = float(t.item())
+    e2e_pageable = {"value": W * world / e2e_p, "unit": UNIT, "h2d_bytes_per_step": n * n * 8,
+                    "d2h_bytes_per_step": 8, "ms_per_step": e2e_p * 1e3, "host_memory": "pageable"}
+    del hpage
 
     if rank == 0:
         peaks = measured_peaks()
@@ -990,8 +1060,8 @@ def main():
         if not args.no_cpu_baseline:
             s = cpu_rank_sample(threads=0, target_s=15.0)
             cpu = {"value": s["value"], "unit": UNIT, "cores": host_cores(), "kind": "port",
-                   "sample": f"oracle rank (src/fp.rs:125-255 restated, OpenMP) of one uniform {s['n']}x{s['n']} "
-                             f"matrix over 2^61-1, {s['seconds']:.1f} s, on {cpu_model()}"}
+                   "sample": f"oracle rank (src/fp.rs:125-255 restated, {oracle_flags}, OpenMP) of one uniform "
+                             f"{s['n']}x{s['n']} matrix over 2^61-1, {s['seconds']:.1f} s, on {cpu_model()}"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -1002,7 +1072,8 @@ def main():
                        "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                        "l2": "inputs (2 GiB) larger than L2", "rank": r, "work_modmac": W,
                        "autotuned": tune},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "parity": parity,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable,
+            "gpu_launches": int(launches), "parity": parity,
             "clocks": clk.summary(), **extras,
         }
         print(json.dumps(line), flush=True)
