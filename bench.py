@@ -353,8 +353,18 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     batch = {"sequences": len(jobs), "total_steps": total, "ms": ms, "steps_per_s": total / (ms * 1e-3),
              "planted_exact": True, "iid_max_dev_from_half": iid_dev}
     g = gold.get(f"lc_batch_{len(jobs)}")
-    if g:
+    if not g and len(jobs) <= 8192:  # no cached answers for this size: the live oracle
+        import oracle
+        host = arena.cpu().numpy().view("uint64")
+        g = {"lcs": [], "macs": 0}
+        for i in range(len(jobs)):
+            o = (ptrs[i] - ptrs[0]) // 8
+            lc_, d_, x_ = oracle.linear_complexity(ps[i], host[o:o + ns[i]], with_macs=True)
+            g["lcs"].append(lc_)
+            g["macs"] += d_ + x_
+    elif g:
         assert arena_digest(arena, ptrs, ns) == g["input_sha256_of_job_sha256"]
+    if g:
         wrong = [i for i in range(len(jobs)) if lcs[i] != g["lcs"][i]]
         assert not wrong, wrong[:5]
         batch["oracle"] = {"all_lcs_equal": True, "sequences_compared": len(jobs), "input_digest_equal": True,
@@ -504,11 +514,21 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    # Every rank against the oracle's (tests/golden/configs.json.gz), whose
-    # column profiles also give the batch's exact modMAC work.
+    # Every rank against the oracle's (tests/golden/configs.json.gz, or the
+    # live oracle for a batch size with no cached answers), whose column
+    # profiles also give the batch's exact modMAC work.
     g = golden_configs().get(f"rank_batch_{len(jobs)}")
-    assert g, "no cached oracle answers for this batch"
-    assert arena_digest(pristine, pptrs, [n * n for n in ns]) == g["input_sha256_of_job_sha256"]
+    if g:
+        assert arena_digest(pristine, pptrs, [n * n for n in ns]) == g["input_sha256_of_job_sha256"]
+    else:
+        import oracle
+        host = pristine.cpu().numpy().view("uint64")
+        g = {"ranks": [], "work_modmac": 0}
+        for i in range(len(jobs)):
+            o = (pptrs[i] - pptrs[0]) // 8
+            r_, pc = oracle.rank(ps[i], host[o:o + ns[i] * ns[i]], ns[i], with_pcols=True)
+            g["ranks"].append(r_)
+            g["work_modmac"] += algorithmic_work(ns[i], pc)
     wrong = [i for i in range(len(jobs)) if ranks[i] != g["ranks"][i]]
     assert not wrong, wrong[:5]
     work_mac = g["work_modmac"]
@@ -660,6 +680,32 @@ def trailing_measure(torch, modlin, n=N, reps=3):
     return res
 
 
+def block_inverse_measure(torch, modlin, calls=4, seed=5):
+    """The 64 x 64 block inverse of the rank's block steps
+    (modlin_block_inverse_device) on a seeded uniform block over 2^61-1:
+    `calls` calls timed with CUDA events, the result checked as P (-P^-1) = -I
+    with exact integers."""
+    from modlin import fp as mfp
+    P = torch.empty(64 * 64, dtype=torch.int64, device="cuda")
+    out = torch.empty(64 * 64, dtype=torch.int64, device="cuda")
+    modlin.gen.uniform_device(M61, seed, P.data_ptr(), 64 * 64)
+    assert mfp.block_inverse_device(M61, P.data_ptr(), 64, out.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(calls):
+        mfp.block_inverse_device(M61, P.data_ptr(), 64, out.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    a = [[int(x) for x in row] for row in P.cpu().numpy().view("uint64").reshape(64, 64)]
+    b = [[int(x) for x in row] for row in out.cpu().numpy().view("uint64").reshape(64, 64)]
+    for i in range(64):
+        for j in range(64):
+            v = sum(a[i][k] * b[k][j] for k in range(64)) % M61
+            assert v == ((M61 - 1) if i == j else 0), (i, j)
+    return {"us_per_call": 1e3 * e0.elapsed_time(e1) / calls, "calls": calls, "check": "P (-P^-1) = -I exactly"}
+
+
 def prng_fill_measure(torch, modlin, count=1 << 32, host_sample=1 << 23, readme_side=65536):
     """The generators' device fill (modlin_prng_fill_device) of the README's
     largest job, 2^32 outputs reduced mod 2^61-1 (a 65536^2 matrix), for
@@ -784,7 +830,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default AUTO choices")
-    ap.add_argument("--workload", default="rank", choices=["rank", "bm", "rank-batch", "rank-planted", "trailing"],
+    ap.add_argument("--batch-count", type=int, default=0,
+                    help="bm / rank-batch workloads: jobs in the batch (default: the full 65536 / 4096)")
+    ap.add_argument("--workload", default="rank",
+                    choices=["rank", "bm", "rank-batch", "rank-planted", "trailing", "block-inverse", "fill"],
                     help="rank: the 16384^2 rank (default line); bm / rank-batch: only those measurements")
     args = ap.parse_args()
 
@@ -808,10 +857,12 @@ def main():
     from modlin import fp as mfp
 
     # The AUTO choices measured on this GPU (a few seconds, before any timing).
-    tune = modlin.autotune()["choice"] if not args.no_autotune and args.workload != "trailing" else None
+    tune = (modlin.autotune()["choice"]
+            if not args.no_autotune and args.workload not in ("trailing", "block-inverse", "fill") else None)
 
     if args.workload == "bm":
-        res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
+        res = bm_measure(torch, modlin, steps=args.steps, warmup=args.warmup,
+                         batch_count=args.batch_count or 65536, cpu=not args.no_cpu_baseline)
         if rank == 0:
             print(json.dumps({"workload": "berlekamp-massey", **res}), flush=True)
         return
@@ -820,13 +871,31 @@ def main():
         if rank == 0:
             print(json.dumps({"workload": "planted large rank", **res}), flush=True)
         return
+    if args.workload == "block-inverse":
+        res = block_inverse_measure(torch, modlin, calls=max(args.steps, 1))
+        print(json.dumps({"workload": "block inverse 64x64 over 2^61-1", **res}), flush=True)
+        return
+    if args.workload == "fill":
+        # MIXMAX-256 device fill of 2^26 outputs mod 2^61-1, `steps` times.
+        g = modlin.prng.Prng("mixmax256", 1)
+        t = torch.empty(1 << 26, dtype=torch.int64, device="cuda")
+        times = []
+        for _ in range(max(args.steps, 1)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            g.fill_device(t.data_ptr(), 1 << 26, M61)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        print(json.dumps({"workload": "MIXMAX-256 device fill, 2^26 outputs mod 2^61-1", "ms": times}), flush=True)
+        return
     if args.workload == "trailing":
         res = trailing_measure(torch, modlin, n=args.n, reps=args.steps)
         if rank == 0:
             print(json.dumps({"workload": "trailing update", **res}), flush=True)
         return
     if args.workload == "rank-batch":
-        res = rank_batch_measure(torch, modlin, steps=args.steps, warmup=args.warmup)
+        res = rank_batch_measure(torch, modlin, steps=args.steps, warmup=args.warmup, count=args.batch_count or 4096)
         if rank == 0:
             print(json.dumps({"workload": "batched rank", **res}), flush=True)
         return
