@@ -353,6 +353,7 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     batch = {"sequences": len(jobs), "total_steps": total, "ms": ms, "steps_per_s": total / (ms * 1e-3),
              "planted_exact": True, "iid_max_dev_from_half": iid_dev}
     g = gold.get(f"lc_batch_{len(jobs)}")
+    cached = bool(g)
     if not g and len(jobs) <= 8192:  # no cached answers for this size: the live oracle
         import oracle
         host = arena.cpu().numpy().view("uint64")
@@ -367,8 +368,8 @@ def bm_measure(torch, modlin, steps=2, warmup=1, long_n=200000, long_L=65280, ba
     if g:
         wrong = [i for i in range(len(jobs)) if lcs[i] != g["lcs"][i]]
         assert not wrong, wrong[:5]
-        batch["oracle"] = {"all_lcs_equal": True, "sequences_compared": len(jobs), "input_digest_equal": True,
-                           "macs": g["macs"]}
+        batch["oracle"] = {"all_lcs_equal": True, "sequences_compared": len(jobs),
+                           "answers": "cached, input digest equal" if cached else "live oracle", "macs": g["macs"]}
         batch["mac_per_s"] = g["macs"] / (ms * 1e-3)
     # Plain form: one sequence per launch, each call waits for its result.
     idx = list(range(0, len(jobs), max(1, len(jobs) // plain_sample)))[:plain_sample]
@@ -518,6 +519,7 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
     # live oracle for a batch size with no cached answers), whose column
     # profiles also give the batch's exact modMAC work.
     g = golden_configs().get(f"rank_batch_{len(jobs)}")
+    cached = bool(g)
     if g:
         assert arena_digest(pristine, pptrs, [n * n for n in ns]) == g["input_sha256_of_job_sha256"]
     else:
@@ -535,7 +537,8 @@ def rank_batch_measure(torch, modlin, steps=2, warmup=1, count=4096, single_samp
     want = [j[3] if j[2] else j[1] for j in jobs]
     res = {"matrices": len(jobs), "ms": ms, "matrices_per_s": len(jobs) / (ms * 1e-3), "work_modmac": work_mac,
            "modmac_per_s": work_mac / (ms * 1e-3),
-           "oracle": {"all_ranks_equal": True, "matrices_compared": len(jobs), "input_digest_equal": True,
+           "oracle": {"all_ranks_equal": True, "matrices_compared": len(jobs),
+                      "answers": "cached, input digest equal" if cached else "live oracle",
                       "non_generic_ranks": sum(1 for i in range(len(jobs)) if ranks[i] != want[i])},
            "step": "restore the 4096 matrices from a pristine copy + one batched call"}
     # The same batch as a plan captured in a CUDA graph: each replay restores
