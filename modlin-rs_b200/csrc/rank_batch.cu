@@ -33,6 +33,29 @@ constexpr int kT = kRankBatchThreads;  // 256
 constexpr int kNW = kT / 32;
 constexpr int kP = 64;  // panel width
 
+// Lazy accumulation of products of residues: u128 sums reduced once per
+// safe_batch products in general; for p < 2^32 a product fits in 32 x 32 ->
+// 64 bits, so the sums stay in a u64 and are reduced once per
+// floor((2^64 - 1) / (p - 1)^2) products (at least 1; p < 2^31 gives >= 4).
+// A reduced sum (< p) counts as one product.
+template <class F>
+struct Acc {
+  using T = u128;
+  __device__ static T prod(const F& f, uint64_t a, uint64_t b) { return f.prod(a, b); }
+  __device__ static uint64_t reduce(const F& f, T x) { return f.reduce(x); }
+  __device__ static uint64_t batch(const F& f) { return f.safe_batch(); }
+};
+template <>
+struct Acc<FpSmall> {
+  using T = uint64_t;
+  __device__ static T prod(const FpSmall&, uint64_t a, uint64_t b) { return (uint64_t)(uint32_t)a * (uint32_t)b; }
+  __device__ static uint64_t reduce(const FpSmall& f, T x) { return f.reduce64(x); }
+  __device__ static uint64_t batch(const FpSmall& f) {
+    const uint64_t q = f.modulus() - 1;
+    return q <= 1 ? UINT64_MAX : UINT64_MAX / (q * q);
+  }
+};
+
 struct BatchSmem {
   uint64_t LF[kP][kP + 1];  // multipliers of a row tile, or the pivot rows' multipliers F[k][k2]
   uint64_t Us[kP][kP];      // U block of one 64-column tile
@@ -47,8 +70,10 @@ struct BatchSmem {
 template <class F>
 __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const int n, int* perm, BatchSmem& S) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  using A = Acc<F>;
+  using AT = typename A::T;
   const uint64_t p = f.modulus();
-  const uint64_t sb = f.safe_batch();
+  const uint64_t sb = A::batch(f);
   for (int i = tid; i < n; i += kT) perm[i] = i;
   __syncthreads();
   int r0 = 0;
@@ -118,17 +143,17 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
           // U_k -= sum_{k2<k} F[k][k2] U_k2, four threads per column.
           const int ci = tid >> 2, q = tid & 3;
           for (int k = 1; k < pb; ++k) {
-            u128 acc = 0;
+            AT acc = 0;
             uint64_t tot = 0, cnt = 0;
             for (int k2 = q; k2 < k; k2 += 4) {
-              acc += f.prod(S.LF[k][k2], S.Us[k2][ci]);
-              if (++cnt == sb) {
-                tot = f.add(tot, f.reduce(acc));
+              acc += A::prod(f, S.LF[k][k2], S.Us[k2][ci]);
+              if (++cnt >= sb) {
+                tot = f.add(tot, A::reduce(f, acc));
                 acc = 0;
                 cnt = 0;
               }
             }
-            uint64_t part = f.add(tot, f.reduce(acc));
+            uint64_t part = f.add(tot, A::reduce(f, acc));
             part = f.add(part, __shfl_xor_sync(0xffffffffu, part, 1));
             part = f.add(part, __shfl_xor_sync(0xffffffffu, part, 2));
             if (q == 0) S.Us[k][ci] = f.sub(S.Us[k][ci], part);
@@ -146,7 +171,7 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
           __syncthreads();
           // A reduced accumulator (< p <= (p-1)^2 + 1) counts as one product,
           // so sb terms never overflow the u128.
-          u128 acc[4][4];
+          AT acc[4][4];
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -161,12 +186,12 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-              for (int q = 0; q < 4; ++q) acc[i][q] += f.prod(a[i], b[q]);
-            if (++cnt == sb) {
+              for (int q = 0; q < 4; ++q) acc[i][q] += A::prod(f, a[i], b[q]);
+            if (++cnt >= sb) {
 #pragma unroll
               for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[i][q] = f.reduce(acc[i][q]);
+                for (int q = 0; q < 4; ++q) acc[i][q] = A::reduce(f, acc[i][q]);
               cnt = 1;
             }
           }
@@ -178,7 +203,7 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const int cc = ct + tx + 16 * q;
-              if (cc < n) R[cc] = f.sub(R[cc], f.reduce(acc[i][q]));
+              if (cc < n) R[cc] = f.sub(R[cc], A::reduce(f, acc[i][q]));
             }
           }
           __syncthreads();
