@@ -109,25 +109,15 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
       const uint64_t* P = m + (int64_t)perm[r] * n + c0;
       if (tid < W) S.prow[tid] = P[tid];
       __syncthreads();
-      // Rows below: a thread per row, so that every thread's loads are in
-      // flight at once (the panel entries of a row are read, updated and
-      // written by its own thread, eight columns at a time).
       const uint64_t inv = S.inv;
-      for (int i = r + 1 + tid; i < n; i += kT) {
+      for (int i = r + 1 + warp; i < n; i += kNW) {
         uint64_t* R = m + (int64_t)perm[i] * n;
         const uint64_t e = R[c];
         if (e == 0) continue;
         const uint64_t fm = f.mul(e, inv);
-        int cc = c + 1;
-        for (; cc + 8 <= c0 + W; cc += 8) {
-          uint64_t v[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) v[u] = R[cc + u];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) R[cc + u] = f.sub(v[u], f.mul(fm, S.prow[cc + u - c0]));
-        }
-        for (; cc < c0 + W; ++cc) R[cc] = f.sub(R[cc], f.mul(fm, S.prow[cc - c0]));
-        R[c] = fm;
+        for (int cc = c + 1 + lane; cc < c0 + W; cc += 32) R[cc] = f.sub(R[cc], f.mul(fm, S.prow[cc - c0]));
+        __syncwarp();
+        if (lane == 0) R[c] = fm;
       }
       __syncthreads();
       ++pb;
