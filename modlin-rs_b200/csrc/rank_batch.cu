@@ -32,6 +32,7 @@ namespace {
 constexpr int kT = kRankBatchThreads;  // 256
 constexpr int kNW = kT / 32;
 constexpr int kP = 64;  // panel width
+constexpr int kG = 4;   // rows per warp in flight during the in-panel elimination
 
 // Lazy accumulation of products of residues: u128 sums reduced once per
 // safe_batch products in general; for p < 2^32 a product fits in 32 x 32 ->
@@ -109,15 +110,31 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
       const uint64_t* P = m + (int64_t)perm[r] * n + c0;
       if (tid < W) S.prow[tid] = P[tid];
       __syncthreads();
+      // Rows below, kG per warp at a time: lane l holds panel entries l and
+      // l + 32 of each of its rows (coalesced loads, all issued before any
+      // is used), so each group costs one memory round trip.
       const uint64_t inv = S.inv;
-      for (int i = r + 1 + warp; i < n; i += kNW) {
-        uint64_t* R = m + (int64_t)perm[i] * n;
-        const uint64_t e = R[c];
-        if (e == 0) continue;
-        const uint64_t fm = f.mul(e, inv);
-        for (int cc = c + 1 + lane; cc < c0 + W; cc += 32) R[cc] = f.sub(R[cc], f.mul(fm, S.prow[cc - c0]));
-        __syncwarp();
-        if (lane == 0) R[c] = fm;
+      const uint64_t pv0 = lane > kk && lane < W ? S.prow[lane] : 0;
+      const uint64_t pv1 = lane + 32 > kk && lane + 32 < W ? S.prow[lane + 32] : 0;
+      for (int base = r + 1 + warp; base < n; base += kNW * kG) {
+        uint64_t* R[kG];
+        uint64_t x0[kG], x1[kG];
+#pragma unroll
+        for (int g = 0; g < kG; ++g) {
+          const int i = base + g * kNW;
+          R[g] = i < n ? m + (int64_t)perm[i] * n + c0 : nullptr;
+          x0[g] = R[g] && lane < W ? R[g][lane] : 0;
+          x1[g] = R[g] && lane + 32 < W ? R[g][lane + 32] : 0;
+        }
+#pragma unroll
+        for (int g = 0; g < kG; ++g) {
+          const uint64_t e = __shfl_sync(0xffffffffu, kk < 32 ? x0[g] : x1[g], kk & 31);
+          if (e == 0) continue;  // uniform across the warp
+          const uint64_t fm = f.mul(e, inv);
+          if (lane > kk && lane < W) R[g][lane] = f.sub(x0[g], f.mul(fm, pv0));
+          if (lane + 32 > kk && lane + 32 < W) R[g][lane + 32] = f.sub(x1[g], f.mul(fm, pv1));
+          if (lane == (kk & 31)) R[g][kk] = fm;
+        }
       }
       __syncthreads();
       ++pb;
