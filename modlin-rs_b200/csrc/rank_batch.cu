@@ -32,7 +32,7 @@ namespace {
 constexpr int kT = kRankBatchThreads;  // 256
 constexpr int kNW = kT / 32;
 constexpr int kP = 64;  // panel width
-constexpr int kG = 4;   // rows per warp in flight during the in-panel elimination
+constexpr int kG = 8;   // rows per warp in flight during the in-panel elimination
 
 // Lazy accumulation of products of residues: u128 sums reduced once per
 // safe_batch products in general; for p < 2^32 a product fits in 32 x 32 ->
@@ -188,6 +188,19 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
           __syncthreads();
           // A reduced accumulator (< p <= (p-1)^2 + 1) counts as one product,
           // so sb terms never overflow the u128.
+          // The tile's C entries are loaded before the products so that
+          // their latency overlaps the arithmetic.
+          uint64_t cv[4][4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int rr = rt + ty + 16 * i;
+            const uint64_t* R = rr < n ? m + (int64_t)perm[rr] * n : nullptr;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int cc = ct + tx + 16 * q;
+              cv[i][q] = R && cc < n ? R[cc] : 0;
+            }
+          }
           AT acc[4][4];
 #pragma unroll
           for (int i = 0; i < 4; ++i)
@@ -220,7 +233,7 @@ __device__ __noinline__ int rank_one(const F& f, uint64_t* __restrict__ m, const
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const int cc = ct + tx + 16 * q;
-              if (cc < n) R[cc] = f.sub(R[cc], A::reduce(f, acc[i][q]));
+              if (cc < n) R[cc] = f.sub(cv[i][q], A::reduce(f, acc[i][q]));
             }
           }
           __syncthreads();
