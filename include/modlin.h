@@ -112,6 +112,16 @@ int modlin_rank_prng(uint64_t p, modlin_prng *g, size_t n, const modlin_rank_opt
 int modlin_trailing_update_device(uint64_t p, uint64_t *d_C, size_t ldc, size_t M, size_t N,
                                   const uint64_t *d_L, const uint64_t *d_U, size_t ldu, size_t K,
                                   int kernel, void *stream);
+/* The pivots of one panel as the reference's in-panel elimination finds
+ * them (src/fp.rs:146-178: per column the first row, in row order, that is
+ * nonzero after the previous pivots' elimination): d_panel is rows x W
+ * (W <= 64, row stride ld >= W) residues in device memory, left unchanged;
+ * *pb_out receives the number of pivots, prow_out[k] / pcol_out[k] (room for
+ * 64 each) the row and the column (0-based, within the panel) of pivot k.
+ * Used by the column-sharded rank for panels whose diagonal block is
+ * singular. Returns when the result is on the host. */
+int modlin_panel_pivots_device(uint64_t p, const uint64_t *d_panel, size_t ld, size_t rows, size_t W,
+                               size_t *prow_out, size_t *pcol_out, size_t *pb_out, void *stream);
 /* The multiplier block of one block step of the rank (the pivot block's
  * inverse; the reference's in-panel elimination, src/fp.rs:146-200, as one
  * device operation): P is 64 x 64 at d_P (row stride ldp >= 64), entries in

@@ -1046,6 +1046,47 @@ static int autotune_locked(Ctx* C, std::string& rep) {
   return MODLIN_OK;
 }
 
+// Pivot structure of one panel (the reference's in-panel elimination,
+// src/fp.rs:146-178): the window and bulk kernels of the general path run on
+// a copy of the rows x W panel, in the panel's row order.
+template <class F>
+static int panel_pivots_locked(Ctx* C, const F& f, const uint64_t* d_panel, size_t ld, size_t rows, size_t W,
+                               size_t* prow_out, size_t* pcol_out, size_t* pb_out, cudaStream_t st) {
+  CK(C->mat.ensure(rows * kPanel * 8));
+  CK(C->lbuf.ensure(std::max(C->lbuf.bytes, rows * kPanel * 8)));
+  CK(C->upanel.ensure((size_t)kPanel * kPanel * 8));
+  CK(C->gmat.ensure((size_t)kPanel * kPanel * 8));
+  CK(C->pstate.ensure(sizeof(PanelState)));
+  CK(C->ispiv.ensure(rows));
+  uint64_t* m = C->mat.as<uint64_t>();
+  CK(cudaMemcpy2DAsync(m, kPanel * 8, d_panel, ld * 8, W * 8, rows, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemsetAsync(C->ispiv.p, 0, rows, st));
+  CK(cudaMemsetAsync(C->pstate.p, 0, sizeof(PanelState), st));
+  PanelState* ps = C->pstate.as<PanelState>();
+  PanelState* h = C->h_ps;
+  const int n = (int)rows;
+  int round = 0, pb_lo = 0;
+  for (;;) {
+    launch_window<F>(f, m, kPanel, n, 0, 0, (int)W, round, ps, C->upanel.as<uint64_t>(), C->gmat.as<uint64_t>(),
+                     C->lbuf.as<uint64_t>(), C->ispiv.as<uint8_t>(), st);
+    launch_bulk<F>(f, m, kPanel, n, 0, 0, (int)W, pb_lo, ps, C->upanel.as<uint64_t>(), C->lbuf.as<uint64_t>(),
+                   C->ispiv.as<uint8_t>(), C->num_sms, st);
+    g_launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h, ps, sizeof(PanelState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h->ncand == 0) break;
+    if (h->pb >= (int)W || ++round > kPanel + 1) return MODLIN_ECUDA;
+    pb_lo = h->pb;
+  }
+  *pb_out = (size_t)h->pb;
+  for (int k = 0; k < h->pb; ++k) {
+    prow_out[k] = (size_t)h->prow[k];
+    pcol_out[k] = (size_t)h->pcol[k];
+  }
+  return MODLIN_OK;
+}
+
 }  // namespace modlin
 
 using namespace modlin;
@@ -1516,6 +1557,24 @@ int modlin_reduce_device(uint64_t p, uint64_t* d_x, size_t count, void* stream) 
   CK(reduce_device(fp, d_x, count, st));
   g_launches++;
   return cuda_rc(cudaStreamSynchronize(st));
+}
+
+int modlin_panel_pivots_device(uint64_t p, const uint64_t* d_panel, size_t ld, size_t rows, size_t W,
+                               size_t* prow_out, size_t* pcol_out, size_t* pb_out, void* stream) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (!pb_out || !prow_out || !pcol_out) return MODLIN_EINVAL_ARG;
+  if (W > (size_t)kPanel || ld < W || rows > 0x3fffffff) return MODLIN_EINVAL_N;
+  *pb_out = 0;
+  if (!rows || !W) return MODLIN_OK;
+  if (!d_panel) return MODLIN_EINVAL_ARG;
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(C->mu);
+  cudaStream_t st = user_stream(stream);
+  if (p == kM61) return panel_pivots_locked(C, FpM61(fp), d_panel, ld, rows, W, prow_out, pcol_out, pb_out, st);
+  return panel_pivots_locked(C, FpBarrett(fp), d_panel, ld, rows, W, prow_out, pcol_out, pb_out, st);
 }
 
 int modlin_block_inverse_device(uint64_t p, const uint64_t* d_P, size_t ldp, uint64_t* d_out, int* singular,

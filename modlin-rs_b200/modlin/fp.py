@@ -230,3 +230,15 @@ def plain_mac_peak(field) -> float:
     out = ctypes.c_double(0)
     check(lib().modlin_plain_mac_peak(_p(field), ctypes.byref(out)), "plain_mac_peak")
     return out.value
+
+
+def panel_pivots_device(field, ptr: int, ld: int, rows: int, W: int, stream: int = 0):
+    """Pivot rows and columns (within the panel) of the rows x W device panel
+    at ``ptr`` (row stride ``ld``), as the reference's in-panel elimination
+    finds them; the panel is not modified."""
+    prow = (szt * 64)()
+    pcol = (szt * 64)()
+    pb = szt(0)
+    check(lib().modlin_panel_pivots_device(_p(field), ptr, ld, rows, W, prow, pcol, ctypes.byref(pb),
+                                           stream or None), "panel_pivots_device")
+    return [int(prow[k]) for k in range(pb.value)], [int(pcol[k]) for k in range(pb.value)]

@@ -70,18 +70,25 @@ def lc_batch_sharded(items, group=None) -> list[int]:
 #
 # The 64-column panels are dealt block-cyclically: panel k lives on process
 # k mod world, each process holding its panels side by side (n rows x its
-# columns, row-major). Block step k, as on one GPU: the diagonal block
-# P = A[64k .. 64k+64, panel k] is inverted by its owner, which forms the
-# multipliers H = X * P^-1 of the rows below (X = those rows' panel entries)
-# and broadcasts H (rows x 64 residues) and whether P was invertible; every
-# process then updates its own panels right of k:
-#     A[rows below, its columns] -= H * A[64k .. 64k+64, its columns].
-# The rank grows by 64 per step. When a diagonal block is singular, or fewer
-# than 64 rows and columns remain, the remaining block (the Schur complement,
-# square) is gathered to process 0 and ranked there by the one-GPU engine,
-# which takes the reference's pivoting path; rank(A) = 64k + its rank, the
-# same invariant as the one-GPU block steps. One broadcast per step, one
-# gather at the end; no device-side waits between processes.
+# columns, row-major). Step k eliminates panel k on the active rows r0 .. n:
+#   * its owner finds the panel's pivots: when the 64 x 64 diagonal block P is
+#     invertible its rows and columns are the pivots (a block step);
+#     otherwise the reference's in-panel elimination (first nonzero row per
+#     column, src/fp.rs:146-178) gives pb <= 64 pivot rows and columns, and
+#     P is the pb x pb block they cross, which is invertible;
+#   * every process moves the pivot rows to the top of the active rows (the
+#     reference's row swaps, src/fp.rs:158-162; none for a block step);
+#   * the owner forms the multipliers of the rows below, H = X P^-1 (X: those
+#     rows' entries in the pivot columns), and broadcasts H (rows x 64);
+#   * every process updates its columns right of panel k:
+#       A[rows below, its columns] -= H * A[pivot rows, its columns],
+#     the Schur complement, whose rank is the rank of what remains.
+# The rank grows by pb per step. Look-ahead: the owner of panel k+1 updates
+# that panel first, finds its pivots and multipliers and starts their
+# broadcast before the rest of its step-k update, so the next step's chain
+# overlaps this step's wide update. Per step the host reads one small header
+# (pivot count, block or general, pivot rows); the buffers are allocated once.
+# No device-side waits between processes, no TMA multicast.
 # ---------------------------------------------------------------------------
 PANEL = 64
 
@@ -110,10 +117,10 @@ def local_columns(n: int, me: int, world: int) -> list[int]:
 
 class DeviceOps:
     """The per-process compute of the sharded rank on this process's GPU,
-    through the C ABI (modlin_block_inverse_device, modlin_trailing_update_
-    device, modlin_rank_device); local blocks are int64 CUDA tensors holding
-    residues. Work is queued on the legacy default stream, so it is ordered
-    with torch's default-stream copies and collectives."""
+    through the C ABI (modlin_block_inverse_device, modlin_panel_pivots_device,
+    modlin_trailing_update_device); local blocks are int64 CUDA tensors
+    holding residues. Work is queued on the legacy default stream, so it is
+    ordered with torch's default-stream copies and collectives."""
 
     def __init__(self, p: int):
         import torch
@@ -121,45 +128,108 @@ class DeviceOps:
             raise RuntimeError("DeviceOps needs a CUDA device")
         self.p = p
         self.torch = torch
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self._X = None
+        self._P = None
+
+    def zeros(self, *shape):
+        return self.torch.zeros(shape, dtype=self.torch.int64, device=self.device)
+
+    def _xbuf(self, rows):
+        if self._X is None or self._X.shape[0] < rows:
+            self._X = self.zeros(max(rows, 1), PANEL)
+        return self._X[:rows]
 
     def block_inverse(self, local, r0: int, c0: int):
-        """-P^-1 of P = local[r0:r0+64, c0:c0+64], or None if P is singular."""
+        """-P^-1 of P = local[r0:r0+64, c0:c0+64] (64 x 64), or None if singular."""
         from .fp import block_inverse_device
-        t = self.torch
-        V = t.empty(PANEL * PANEL, dtype=t.int64, device=local.device)
+        if self._P is None:
+            self._P = self.zeros(2, PANEL * PANEL)
+        V = self._P[0]
         ld = local.shape[1]
         ok = block_inverse_device(self.p, local.data_ptr() + 8 * (r0 * ld + c0), ld, V.data_ptr())
         return V if ok else None
 
-    def multipliers(self, local, r0: int, c0: int, Vneg):
-        """H = X * P^-1 = 0 - X * (-P^-1), X = local[r0+64:, c0:c0+64]."""
+    def panel_pivots(self, local, r0: int, c0: int, W: int):
+        """Pivot rows (relative to r0) and columns (within the panel) of
+        local[r0:, c0:c0+W]."""
+        from .fp import panel_pivots_device
+        ld = local.shape[1]
+        return panel_pivots_device(self.p, local.data_ptr() + 8 * (r0 * ld + c0), ld, local.shape[0] - r0, W)
+
+    def sub_inverse(self, local, rows, cols):
+        """-P^-1 embedded in 64 x 64 ([[P, 0], [0, I]]) for P = local[rows][:, cols]."""
+        from .fp import block_inverse_device
+        t = self.torch
+        pb = len(rows)
+        P = self.zeros(PANEL, PANEL)
+        P[pb:, pb:] = t.eye(PANEL - pb, dtype=t.int64, device=self.device)
+        ri = t.tensor(rows, device=self.device)
+        ci = t.tensor(cols, device=self.device)
+        P[:pb, :pb] = local.index_select(0, ri).index_select(1, ci)
+        V = self._P[1] if self._P is not None else self.zeros(PANEL * PANEL)
+        if not block_inverse_device(self.p, P.data_ptr(), PANEL, V.data_ptr()):
+            raise RuntimeError("pivot block of a panel is singular")
+        return V
+
+    def multipliers(self, local, r0: int, rows_below, cols, V, out):
+        """out[:m] = X P^-1 = 0 - X (-P^-1), X = local[rows_below][:, cols]
+        padded to 64 columns; rows_below is a range (block step) or a list."""
         from .fp import trailing_update_device
         t = self.torch
-        X = local[r0 + PANEL:, c0:c0 + PANEL].contiguous()
-        H = t.zeros_like(X)
-        if X.shape[0]:
-            trailing_update_device(self.p, H.data_ptr(), PANEL, X.shape[0], PANEL, X.data_ptr(), Vneg.data_ptr(),
-                                   PANEL, PANEL, kernel="auto")
+        m = len(rows_below)
+        X = self._xbuf(m)
+        if isinstance(rows_below, range) and len(cols) == PANEL and cols[-1] - cols[0] == PANEL - 1:
+            X.copy_(local[rows_below.start:rows_below.stop, cols[0]:cols[0] + PANEL])
+        else:
+            X.zero_()
+            if m:
+                ri = t.tensor(list(rows_below), device=self.device)
+                ci = t.tensor(cols, device=self.device)
+                X[:, :len(cols)] = local.index_select(0, ri).index_select(1, ci)
+        H = out[:m]
+        H.zero_()
+        if m:
+            trailing_update_device(self.p, H.data_ptr(), PANEL, m, PANEL, X.data_ptr(), V.data_ptr(), PANEL, PANEL,
+                                   kernel="auto")
         return H
 
-    def empty_h(self, rows: int, like):
-        return self.torch.empty((rows, PANEL), dtype=self.torch.int64, device=like.device)
+    def move_rows(self, local, r0: int, perm):
+        """Rows r0.. of local take the order perm (absolute row indices)."""
+        t = self.torch
+        local[r0:] = local.index_select(0, t.tensor(perm, device=self.device))
 
-    def update(self, local, r0: int, cstart: int, H):
-        """local[r0+64:, cstart:] -= H * local[r0:r0+64, cstart:]."""
+    def update(self, local, r0: int, pb: int, c_from: int, c_to: int, H):
+        """local[r0+pb:, c_from:c_to] -= H[:, :pb] * local[r0:r0+pb, c_from:c_to]."""
         from .fp import trailing_update_device
         ld = local.shape[1]
-        M, N = local.shape[0] - r0 - PANEL, ld - cstart
-        if M > 0 and N > 0:
-            trailing_update_device(self.p, local.data_ptr() + 8 * ((r0 + PANEL) * ld + cstart), ld, M, N,
-                                   H.data_ptr(), local.data_ptr() + 8 * (r0 * ld + cstart), ld, PANEL, kernel="auto")
+        M, N = local.shape[0] - r0 - pb, c_to - c_from
+        if M > 0 and N > 0 and pb > 0:
+            trailing_update_device(self.p, local.data_ptr() + 8 * ((r0 + pb) * ld + c_from), ld, M, N,
+                                   H.data_ptr(), local.data_ptr() + 8 * (r0 * ld + c_from), ld, pb, kernel="auto")
 
-    def rank(self, block) -> int:
-        """Rank of a square block (clobbered) on this GPU."""
-        from .fp import rank_device
-        n = block.shape[0]
-        block = block.contiguous()
-        return rank_device(self.p, block.data_ptr(), n) if n else 0
+
+def _factor(ops, local, n, r0, c0, W, out):
+    """The owner's part of a step on panel columns c0 .. c0+W of its block:
+    (pb, block_step, pivot rows in their new order, H = multipliers of the
+    rows below, in the new row order)."""
+    rows_active = n - r0
+    if rows_active <= 0:
+        return 0, True, [], out[:0]
+    if W == PANEL and rows_active >= PANEL:
+        V = ops.block_inverse(local, r0, c0)
+        if V is not None:
+            H = ops.multipliers(local, r0, range(r0 + PANEL, n), list(range(c0, c0 + PANEL)), V, out)
+            return PANEL, True, list(range(r0, r0 + PANEL)), H
+    prow, pcol = ops.panel_pivots(local, r0, c0, W)
+    pb = len(prow)
+    if pb == 0:
+        return 0, False, [], out[:0]
+    piv = [r0 + r for r in prow]
+    below = [r for r in range(r0, n) if r not in set(piv)]
+    V = ops.sub_inverse(local, piv, [c0 + c for c in pcol])
+    H = ops.multipliers(local, r0, below, [c0 + c for c in pcol], V, out)
+    return pb, False, piv, H
 
 
 def rank_sharded(p: int, local, n: int, ops=None, group=None) -> int:
@@ -176,74 +246,87 @@ def rank_sharded(p: int, local, n: int, ops=None, group=None) -> int:
     world = dist.get_world_size(group) if dist_on else 1
     me = dist.get_rank(group) if dist_on else 0
     mine = local_panels(n, me, world)
+    pos = {q: i for i, q in enumerate(mine)}
     npan = (n + PANEL - 1) // PANEL
-    dev = local.device
+    width = local.shape[1]
 
-    def bcast(t, src):
-        if world > 1:
-            dist.broadcast(t, src=dist.get_global_rank(group, src) if group is not None else src, group=group)
-        return t
+    def src(r):
+        return dist.get_global_rank(group, r) if group is not None else r
 
-    rank, k = 0, 0
-    while k < npan and panel_width(n, k) == PANEL and n - PANEL * k >= PANEL:
-        r0 = PANEL * k
+    def bcast(t, owner):
+        if world == 1:
+            return None
+        return dist.broadcast(t, src=src(owner), group=group, async_op=True)
+
+    # Header: [pb, block step, pivot rows (64)]; two multiplier buffers so
+    # that a send can still be in flight while the next step's is formed.
+    hdr = [ops.zeros(2 + PANEL) for _ in range(2)]
+    Hbuf = [ops.zeros(max(n, 1), PANEL) for _ in range(2)]
+    pending = [[], []]  # sends still in flight from each buffer pair
+
+    def lead(k, r0):
+        """Owner of panel k: factor it; everyone: exchange its header and
+        multipliers. Returns (pb, block, pivot rows, H, H work)."""
+        b = k & 1
+        for w in pending[b]:
+            w.wait()
+        pending[b] = []
         owner = panel_owner(k, world)
-        rows = n - r0 - PANEL
-        H = None
-        flag = torch.zeros(1, dtype=torch.int64, device=dev)
         if me == owner:
-            c0 = PANEL * mine.index(k)
-            V = ops.block_inverse(local, r0, c0)
-            if V is not None:
-                flag.fill_(1)
-                H = ops.multipliers(local, r0, c0, V)
-        bcast(flag, owner)
-        if int(flag.item()) == 0:
-            break
-        if H is None:
-            H = ops.empty_h(rows, local)
-        if rows:
-            bcast(H, owner)
-        # This process's panels right of k start at local panel index j0.
+            c0 = PANEL * pos[k]
+            pb, block, piv, H = _factor(ops, local, n, r0, c0, panel_width(n, k), Hbuf[b])
+            vals = [pb, int(block)] + piv + [0] * (PANEL - len(piv))
+            hdr[b].copy_(torch.tensor(vals, dtype=torch.int64))
+        w = bcast(hdr[b], owner)
+        if w is not None:
+            if me == owner:
+                pending[b].append(w)
+            else:
+                w.wait()
+        h = hdr[b].tolist()
+        pb, block, piv = int(h[0]), bool(h[1]), [int(x) for x in h[2:2 + int(h[0])]]
+        rows = n - r0 - pb
+        H = Hbuf[b][:max(rows, 0)]
+        wh = bcast(H, owner) if pb > 0 and rows > 0 else None
+        if me == owner:
+            if wh is not None:
+                pending[b].append(wh)  # the buffer is reused two steps later
+            wh = None
+        return pb, block, piv, H, wh
+
+    r0, k = 0, 0
+    cur = lead(0, 0) if npan else None
+    while k < npan and r0 < n:
+        pb, block, piv, H, wh = cur
+        if pb > 0 and not block:
+            below = [r for r in range(r0, n) if r not in set(piv)]
+            ops.move_rows(local, r0, piv + below)
+        if wh is not None:
+            wh.wait()
+        # Local columns right of panel k.
         j0 = sum(1 for q in mine if q <= k)
-        ops.update(local, r0, PANEL * j0, H)
-        rank += PANEL
-        k += 1
-    # The rest: the square block rows r0.., columns of panels >= k.
-    r0 = PANEL * k
-    rest = n - r0
-    if rest > 0:
-        j0 = sum(1 for q in mine if q < k)
-        part = local[r0:, PANEL * j0:].contiguous()
-        if world > 1:
-            widths = [len(local_columns(n, r, world)) - PANEL * sum(1 for q in local_panels(n, r, world) if q < k)
-                      for r in range(world)]
-            wmax = max(widths)
-            pad = torch.zeros((rest, wmax), dtype=torch.int64, device=dev)
-            pad[:, :part.shape[1]] = part
-            parts = [torch.empty_like(pad) for _ in range(world)] if me == 0 else None
-            dst = dist.get_global_rank(group, 0) if group is not None else 0
-            dist.gather(pad, parts, dst=dst, group=group)
-            if me == 0:
-                cols = [parts[r][:, :widths[r]] for r in range(world)]
-                # Reassemble global column order: panel q >= k is the next
-                # PANEL columns of process q mod world.
-                pos = [0] * world
-                blocks = []
-                for q in range(k, npan):
-                    r = panel_owner(q, world)
-                    w = panel_width(n, q)
-                    blocks.append(cols[r][:, pos[r]:pos[r] + w])
-                    pos[r] += w
-                block = torch.cat(blocks, dim=1)
+        c_from = PANEL * j0
+        nxt_owner = panel_owner(k + 1, world) if k + 1 < npan else -1
+        r1 = r0 + pb
+        if nxt_owner == me and pb > 0 and r1 < n:
+            # Look-ahead: panel k+1 first, then its factorization and the
+            # start of its broadcast, then the rest of this step's update.
+            c1 = PANEL * pos[k + 1]
+            ops.update(local, r0, pb, c1, c1 + panel_width(n, k + 1), H)
+            nxt = lead(k + 1, r1)
+            ops.update(local, r0, pb, c1 + panel_width(n, k + 1), width, H)
         else:
-            block = part
-        res = torch.zeros(1, dtype=torch.int64, device=dev)
-        if me == 0:
-            res.fill_(ops.rank(block))
-        bcast(res, 0)
-        rank += int(res.item())
-    return rank
+            if pb > 0:
+                ops.update(local, r0, pb, c_from, width, H)
+            nxt = lead(k + 1, r1) if k + 1 < npan and r1 < n else None
+        r0, k = r1, k + 1
+        cur = nxt
+        if cur is None:
+            break
+    for ws in pending:
+        for w in ws:
+            w.wait()
+    return r0
 
 
 def scatter_columns(a, n: int, me: int, world: int):

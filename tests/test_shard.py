@@ -91,7 +91,7 @@ def test_run_sharded_gloo_world2(O):
 # ---- the column-sharded single rank ------------------------------------------
 
 SHARD_CASES = [("uniform", M61, 200, 0), ("planted", M61, 200, 100), ("uniform", 2, 150, 0),
-               ("uniform", 65521, 130, 0), ("uniform", M61, 40, 0)]
+               ("uniform", 65521, 130, 0), ("uniform", M61, 40, 0), ("planted", 97, 170, 120)]
 
 
 def _case_matrix(O, kind, p, n, L):
@@ -110,24 +110,32 @@ def test_sharded_rank_one_process(O):
     import torch
     from modlin.shard import rank_sharded, scatter_columns
     from shard_host_ops import HostOps
+
     class Counting(HostOps):
-        steps = 0
+        blocks = general = 0
 
-        def multipliers(self, *a):
-            Counting.steps += 1
-            return super().multipliers(*a)
+        def block_inverse(self, *a):
+            r = super().block_inverse(*a)
+            Counting.blocks += r is not None
+            return r
 
-    # Block steps taken: every full panel of the uniform matrix over 2^61-1;
-    # one for the planted rank-100 matrix (its second diagonal block lies in
-    # a rank-36 Schur complement, so the rest is gathered there).
-    steps = {("uniform", M61, 200): 3, ("planted", M61, 200): 1, ("uniform", M61, 40): 0}
+        def panel_pivots(self, *a):
+            Counting.general += 1
+            return super().panel_pivots(*a)
+
+    # Steps taken: block steps on every full panel of the uniform matrix over
+    # 2^61-1 and general steps on its ragged last panel; the planted rank-100
+    # matrix takes one block step and then general steps on the panels of its
+    # rank-36 Schur complement (no gather of the remaining block).
+    steps = {("uniform", M61, 200): (3, 1), ("planted", M61, 200): (1, 3), ("uniform", M61, 40): (0, 1)}
     for kind, p, n, L in SHARD_CASES:
         a = _case_matrix(O, kind, p, n, L)
         local = torch.from_numpy(scatter_columns(a, n, 0, 1).view(np.int64))
-        Counting.steps = 0
+        Counting.blocks = Counting.general = 0
         assert rank_sharded(p, local, n, ops=Counting(p, O)) == O.rank(p, a, n), (kind, p, n)
         if (kind, p, n) in steps:
-            assert Counting.steps == steps[(kind, p, n)], (kind, p, n, Counting.steps)
+            assert (Counting.blocks, Counting.general) == steps[(kind, p, n)], (kind, p, n, Counting.blocks,
+                                                                               Counting.general)
 
 
 def _shard_worker(rank, world, port, q):
@@ -158,9 +166,10 @@ def _shard_worker(rank, world, port, q):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_sharded_rank_gloo(O, world):
-    """Column panels dealt over `world` processes, one broadcast of the
-    multipliers per block step, the remaining block gathered and ranked at
-    the end: every process returns the oracle's rank."""
+    """Column panels dealt over `world` processes, the panel owner's pivots
+    and multipliers broadcast per step (block steps, pivoted general steps,
+    look-ahead on the next panel's owner): every process returns the
+    oracle's rank."""
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.SimpleQueue()
