@@ -822,6 +822,63 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded_rank(args, torch, dist, modlin, rank, world, local):
+    """One n x n rank over 2^61-1 with its 64-column panels dealt
+    block-cyclically over the `world` processes (modlin.shard.rank_sharded):
+    strong scaling, total work fixed. Each step regenerates this process's
+    columns of the SplitMix64(7) matrix from a device copy; the time is the
+    max over ranks of CUDA-event time around the rank."""
+    import numpy as np
+    from modlin import shard
+    n = args.n
+    full = torch.empty(n * n, dtype=torch.int64, device="cuda")
+    modlin.gen.uniform_device(M61, 7, full.data_ptr(), n * n)
+    cols = torch.tensor(shard.local_columns(n, rank, world), device="cuda")
+    pristine = full.view(n, n).index_select(1, cols).contiguous()
+    del full
+    torch.cuda.empty_cache()
+    work = torch.empty_like(pristine)
+    ops = shard.DeviceOps(M61)
+
+    def step():
+        work.copy_(pristine)
+        return shard.rank_sharded(M61, work, n, ops=ops)
+
+    for _ in range(args.warmup):
+        r = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        r = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    W = algorithmic_work(n, range(r))
+    g = golden_configs().get(f"rank_uniform_{n}")
+    if g:
+        assert r == g["rank"], (r, g["rank"])
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": W / (ms_per_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "u64 (INT8 limbs on the tensor cores)", "data": "synthetic",
+            "config": {"workload": f"one rank {n}x{n} over p=2^61-1, uniform SplitMix64(7) residues, column panels "
+                                   f"dealt over {world} GPU(s)", "n": n, "p": M61, "rank": r, "work_modmac": W,
+                       "parallelism": f"column-sharded x{world}", "l2": "inputs larger than L2"},
+            "parity": {"oracle_rank": g["rank"] if g else None}}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -833,6 +890,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default AUTO choices")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "sharded"],
+                    help="N > 1 GPUs: independent replicas of the rank (weak scaling, default) or one rank "
+                         "with its column panels dealt over the GPUs (strong scaling, modlin.shard.rank_sharded)")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="bm / rank-batch workloads: jobs in the batch (default: the full 65536 / 4096)")
     ap.add_argument("--workload", default="rank",
@@ -902,6 +962,9 @@ def main():
         if rank == 0:
             print(json.dumps({"workload": "batched rank", **res}), flush=True)
         return
+
+    if args.mode == "sharded":
+        return run_sharded_rank(args, torch, dist, modlin, rank, world, local)
 
     n = args.n
     kernel = args.kernel

@@ -103,6 +103,16 @@ int modlin_rank_device(uint64_t p, uint64_t *d_m, size_t n, const modlin_rank_op
 int modlin_rank_prng(uint64_t p, modlin_prng *g, size_t n, const modlin_rank_opts *opts, size_t *rank_out,
                      modlin_progress_fn cb, void *cb_ctx);
 
+/* The CLI's -R loop over `reps` matrices (src/main.rs:82-125) in batched
+ * launches: the next reps * n*n outputs of g, reduced mod p, fill reps
+ * matrices in device memory (row-major, one after another: the same matrices
+ * as reps calls of modlin_rank_prng) and their ranks go to ranks_out[0..reps)
+ * from one persistent launch per group of matrices that fits 8 GiB. Sides
+ * above 8192 (and reps == 1) run one matrix at a time. cb (may be NULL)
+ * receives matrices done / reps. */
+int modlin_rank_prng_batch(uint64_t p, modlin_prng *g, size_t n, size_t reps, const modlin_rank_opts *opts,
+                           size_t *ranks_out, modlin_progress_fn cb, void *cb_ctx);
+
 /* The trailing update of one panel (src/fp.rs:202-248) as a standalone
  * device operation: C[M x N] -= L[M x K] * U[K x N] (mod p), all entries in
  * [0, p). K <= 64 (L row stride 64), or with the tensor-core kernel also

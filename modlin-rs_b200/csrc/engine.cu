@@ -89,6 +89,7 @@ struct Ctx {
   std::mutex mu;
   // rank workspaces
   DevBuf mat, lbuf, ubuf, upanel, gmat, pstate, ispiv, moves;
+  DevBuf repsbuf;  // matrices of a batched -R run
   DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
   DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
   DevBuf binv;      // block-step status words and the negated block inverse
@@ -1632,6 +1633,48 @@ int modlin_rank_prng(uint64_t p, modlin_prng* g, size_t n, const modlin_rank_opt
   g_launches += nl;
   if (rc) return rc;
   return rank_device_locked(C, p, C->mat.as<uint64_t>(), n, opts, rank_out, nullptr, C->stream, cb, cb_ctx);
+}
+
+int modlin_rank_prng_batch(uint64_t p, modlin_prng* g, size_t n, size_t reps, const modlin_rank_opts* opts,
+                           size_t* ranks_out, modlin_progress_fn cb, void* cb_ctx) {
+  FieldParams fp;
+  if (!make_field_params(p, &fp)) return MODLIN_EINVAL_P;
+  if (n == 0 || n > 0x7fffffff / 2 || n > SIZE_MAX / n / 8) return MODLIN_EINVAL_N;
+  if (!g || (reps && !ranks_out)) return MODLIN_EINVAL_ARG;
+  if (reps == 0) return MODLIN_OK;
+  if (reps == 1 || (int64_t)n > kRankBatchMaxN) {
+    for (size_t i = 0; i < reps; ++i) {
+      const int rc = modlin_rank_prng(p, g, n, opts, ranks_out + i, nullptr, nullptr);
+      if (rc) return rc;
+      if (cb) cb(cb_ctx, i + 1, reps);
+    }
+    return MODLIN_OK;
+  }
+  Ctx* C = nullptr;
+  int rc = get_ctx(&C);
+  if (rc) return rc;
+  std::unique_lock<std::mutex> lk(C->mu);
+  const size_t per = n * n;
+  const size_t budget = (size_t)8 << 30;  // bytes of matrices in flight at once
+  const size_t chunk = std::max<size_t>(1, std::min(reps, budget / (per * 8)));
+  CK(C->repsbuf.ensure(chunk * per * 8));
+  uint64_t* arena = C->repsbuf.as<uint64_t>();
+  std::vector<uint64_t> ps(chunk, p);
+  std::vector<size_t> ns(chunk, n);
+  std::vector<uint64_t*> ptrs(chunk);
+  for (size_t i = 0; i < chunk; ++i) ptrs[i] = arena + i * per;
+  for (size_t done = 0; done < reps; done += chunk) {
+    const size_t c = std::min(chunk, reps - done);
+    uint64_t nl = 0;
+    rc = prng_fill_device(C->prng, C->num_sms, g, p, fp, arena, (uint64_t)(c * per), C->stream, &nl);
+    g_launches += nl;
+    if (rc) return rc;
+    rc = rank_batch_locked(C, ps.data(), ptrs.data(), ns.data(), c, ranks_out + done, C->stream, lk,
+                           opts ? opts->kernel : MODLIN_RANK_AUTO);
+    if (rc) return rc;
+    if (cb) cb(cb_ctx, done + c, reps);
+  }
+  return MODLIN_OK;
 }
 
 uint64_t modlin_kernel_launches(void) { return g_launches.load(); }

@@ -246,8 +246,9 @@ int main(int argc, char** argv) {
                 format_memory((double)n * n * 8).c_str(), reps, n, n, reps == 1 ? "matrix" : "matrices", modulus);
     std::fflush(stdout);
     // Each matrix is the next n*n outputs reduced mod p (src/main.rs:94-104),
-    // generated in device memory and ranked there.
-    for (uint64_t i = 0; i < reps; ++i) {
+    // generated in device memory and ranked there; several reps go into
+    // batched launches (the printed results are the same as one at a time).
+    if (reps == 1) {
       const auto t0 = std::chrono::steady_clock::now();
       size_t r = 0;
       const int rc = modlin_rank_prng(modulus, rng, n, &ropts, &r, progress_cb, &pr);
@@ -256,12 +257,27 @@ int main(int argc, char** argv) {
         return 1;
       }
       const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      std::fprintf(stderr, "Matrix %" PRIu64 "/%" PRIu64 ": generated and ranked in %.3f ms\n", i + 1, reps, ms);
+      std::fprintf(stderr, "Matrix 1/1: generated and ranked in %.3f ms\n", ms);
       const size_t corank = n - r;
-      std::printf("Matrix %" PRIu64 "/%" PRIu64 "\tcorank=%zu\tp=%s\n", i + 1, reps, corank,
+      std::printf("Matrix 1/1\tcorank=%zu\tp=%s\n", corank,
                   pretty(modlin_corank_tail_pvalue(modulus, n, corank)).c_str());
-      std::fflush(stdout);
+    } else {
+      std::vector<size_t> ranks(reps);
+      const auto t0 = std::chrono::steady_clock::now();
+      const int rc = modlin_rank_prng_batch(modulus, rng, n, reps, &ropts, ranks.data(), nullptr, nullptr);
+      if (rc) {
+        std::fprintf(stderr, "rank failed: %s\n", modlin_strerror(rc));
+        return 1;
+      }
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      std::fprintf(stderr, "%" PRIu64 " matrices generated and ranked in %.3f ms\n", reps, ms);
+      for (uint64_t i = 0; i < reps; ++i) {
+        const size_t corank = n - ranks[i];
+        std::printf("Matrix %" PRIu64 "/%" PRIu64 "\tcorank=%zu\tp=%s\n", i + 1, reps, corank,
+                    pretty(modlin_corank_tail_pvalue(modulus, n, corank)).c_str());
+      }
     }
+    std::fflush(stdout);
   } else {  // src/main.rs:135-176
     const size_t n = length;
     std::printf("Running a modular linear-complexity test using %s of RAM: %" PRIu64 " %s of length %zu over the field of size %" PRIu64 "\n",

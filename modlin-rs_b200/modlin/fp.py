@@ -108,6 +108,16 @@ def rank_prng(field, gen, n: int, *, kernel: str = "auto", progress=None) -> int
     return int(out.value)
 
 
+def rank_prng_batch(field, gen, n: int, reps: int, *, kernel: str = "auto") -> list[int]:
+    """Ranks of the next ``reps`` n x n matrices of ``gen``'s outputs reduced
+    mod p (the CLI's -R reps loop, src/main.rs:82-125), in batched launches."""
+    opts = RankOpts(KERNELS[kernel], 0)
+    out = (szt * max(reps, 1))()
+    check(lib().modlin_rank_prng_batch(_p(field), gen.handle, n, reps, ctypes.byref(opts), out, _NO_PROGRESS,
+                                       None), "rank_prng_batch")
+    return [int(out[i]) for i in range(reps)]
+
+
 def linear_complexity(field, s, *, kernel: str = "auto", grid_ctas: int = 0, check_input: bool = False) -> int:
     """``fp::linear_complexity`` (src/fp.rs:260)."""
     a = _as_u64(s)

@@ -74,3 +74,20 @@ def test_readme_headline_mixmax256_rank_65536():
     out = run("-R", "65536", "-p", str(M61), "-S", "1", "--prng", "mixmax256")
     assert out[0] == "Generator: MIXMAX (TRandomMixMax256, N=256, skip=2)"
     assert out[-1] == "Matrix 1/1\tcorank=256\tp=1e-307"
+
+
+def test_rank_reps_batched_equal_one_at_a_time(M, O):
+    """-R with several reps runs them in batched launches; every matrix is
+    the next n*n outputs of the generator, so the results equal the oracle's
+    ranks of consecutive slices of the host stream (src/main.rs:82-125)."""
+    n, reps = 120, 5
+    for p in (M61, 2, 97):
+        out = run("-R", str(n), "-p", str(p), "-S", "7", "--prng", "mixmax17", str(reps))
+        stream = O.prng("mixmax17", 7, reps * n * n)
+        F = O.Field(p)
+        for i in range(reps):
+            m = [F.reduce(int(x)) for x in stream[i * n * n:(i + 1) * n * n]]
+            corank = n - O.rank(p, m, n)
+            assert out[3 + i].startswith(f"Matrix {i + 1}/{reps}\tcorank={corank}\tp="), (p, i, out[3 + i])
+    g = M.prng.Prng("mixmax17", 7)
+    assert M.fp.rank_prng_batch(M61, g, n, reps) == [n] * reps
