@@ -318,6 +318,12 @@ uint64_t modlin_kernel_launches(void);
  * multiply-adds per second (best of three timed launches). No reference
  * counterpart: it is the denominator of the plain kernel's pipe fraction. */
 int modlin_plain_mac_peak(uint64_t p, double *modmac_per_s);
+/* Tensor-core updates over 2^61 - 1 run on CTA pairs (thread-block clusters
+ * of two CTAs sharing each B tile, M = 256 MMAs) when enable = 1 (the
+ * default) or on single CTAs when enable = 0; enable < 0 only queries.
+ * Returns the previous setting. Both kernels give the same, exact results;
+ * no reference counterpart (a kernel choice, like MODLIN_RANK_TC). */
+int modlin_set_tc_pairs(int enable);
 /* Failure-detection test hook (no reference counterpart; the reference has
  * no device waits): the next MODLIN_LC_GRID launch in this process bounds
  * each grid-barrier wait by spin_cycles (1 .. 4e9) instead of ~1 s, and its

@@ -1679,6 +1679,12 @@ int modlin_rank_prng_batch(uint64_t p, modlin_prng* g, size_t n, size_t reps, co
 
 uint64_t modlin_kernel_launches(void) { return g_launches.load(); }
 
+int modlin_set_tc_pairs(int enable) {
+  const int prev = g_tc_pairs ? 1 : 0;
+  if (enable >= 0) g_tc_pairs = enable != 0;
+  return prev;
+}
+
 int modlin_testing_grid_timeout_once(long long spin_cycles, int skip_cta) {
   if (spin_cycles < 1 || spin_cycles > 4000000000LL || skip_cta < 0) return MODLIN_EINVAL_ARG;
   g_fault_spin.store(spin_cycles);

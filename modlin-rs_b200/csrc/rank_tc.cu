@@ -671,6 +671,287 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same update over 2^61 - 1 on CTA pairs (cta_group::2, cluster of 2):
+// the pair computes 256-row x 16-column subtiles with M = 256 MMAs issued by
+// the even CTA; each CTA keeps its own 128 rows of A resident and streams its
+// half of every B subtile (limb planes 0..3 in the even CTA, 4..7 in the odd
+// one), so each SM reads 6 KB of operands from shared memory per 64 tensor
+// cycles instead of 8 KB. Each CTA's TMEM holds its rows' accumulators; its
+// epilogue is the 1-CTA kernel's (two 8-warp groups, C by 2D TMA). The even
+// CTA's MMA thread learns that the odd CTA's copies have landed from that
+// CTA's relay thread (a remote mbarrier arrive), and the odd CTA's epilogue
+// releases TMEM buffers by remote arrives; MMA completions reach both CTAs
+// through multicast commits. The upper diagonal blocks 8..14 are zeroed by
+// the epilogue (TMEM stores) after it drains a buffer, and once at start.
+// ---------------------------------------------------------------------------
+template <int KK>
+struct PairShape {
+  static constexpr int NS = 16;
+  static constexpr int TILE = 128 * KK;  // one limb plane of 128 rows
+  static constexpr int KC = KK / 16;
+  static constexpr uint32_t SBO = KK * 8;
+  static constexpr int A_BYTES = 8 * TILE;   // this CTA's 128 rows, 8 planes
+  static constexpr int BH_BYTES = 4 * 16 * KK;  // half a B subtile: 4 limb planes x 16 columns x KK
+  static constexpr int STAGES = KK == 64 ? 8 : 6;
+  static constexpr int C_BYTES = 2 * 128 * 16 * 8;
+  static constexpr int SMEM = A_BYTES + STAGES * BH_BYTES + 1024 + C_BYTES;
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+template <int KK>
+__global__ void __launch_bounds__(kThreads, 1)
+    trailing_tc_pair_kernel(const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, int32_t rbeg,
+                            int32_t jend, Sched S, int* err, const __grid_constant__ CUtensorMap cmap) {
+  using SH = PairShape<KK>;
+  constexpr int NS = SH::NS;
+  constexpr int kStages = SH::STAGES;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + SH::A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kStages * SH::BH_BYTES);
+  uint64_t* sC = bars + 128;  // 1 KB of barriers, then the C tiles (1024-byte aligned)
+  uint64_t* a_full = bars + 0;
+  uint64_t* a_empty = bars + 1;
+  uint64_t* acc_full = bars + 2;   // [2]
+  uint64_t* acc_empty = bars + 4;  // [2], even CTA: 8 local + 8 remote arrivals
+  uint64_t* mma_done = bars + 6;
+  uint64_t* a_peer = bars + 7;     // even CTA: the odd CTA's A tile has landed
+  uint64_t* b_full = bars + 8;
+  uint64_t* b_empty = bars + 8 + kStages;
+  uint64_t* b_peer = bars + 8 + 2 * kStages;  // even CTA: the odd CTA's B half has landed
+  __shared__ uint32_t tmem_base_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t crank = cluster_rank();
+  const int pair = blockIdx.x >> 1;
+  const int npairs = gridDim.x >> 1;
+  if (threadIdx.x == 0) {
+    mbar_init(a_full, 1);
+    mbar_init(a_empty, 1);
+    mbar_init(a_peer, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + b, 1);
+      mbar_init(acc_empty + b, kEpiWarps);  // both CTAs' group of 8 warps
+    }
+    mbar_init(mma_done, 1);
+    mbar_init(bars + 40, 1);  // c_full of epilogue group 0
+    mbar_init(bars + 41, 1);  // c_full of epilogue group 1
+    for (int st = 0; st < kStages; ++st) {
+      mbar_init(b_full + st, 1);
+      mbar_init(b_empty + st, 1);
+      mbar_init(b_peer + st, 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if (warp >= 2) {
+    // Zero the upper diagonal blocks (8 .. 14) of this group's buffer.
+    const int ew = warp - 2, grp = ew >> 3, quad = warp & 3, half = (ew >> 2) & 1;
+    const uint32_t lb = tmem + ((uint32_t)(quad * 32) << 16) + grp * 256 + half * 8;
+#pragma unroll
+    for (int d = 8; d < 15; ++d) tmem_st8_zero(lb + d * NS);
+    tmem_wait_st();
+  }
+  fence_before();
+  cluster_sync_all();  // both CTAs' barriers initialised and their buffers zeroed
+  fence_after();
+  const int64_t total = (int64_t)S.mtiles * S.nsub;  // (256-row tile, subtile) pairs
+  const int64_t g0 = total * pair / npairs, g1 = total * (pair + 1) / npairs;
+
+  if (warp == 0) {
+    // ---------------- producer (both CTAs): this CTA's A rows and B half ----
+    if (lane == 0) {
+      int cur = -1, nload = 0, it = 0;
+      int64_t mt = g0 / S.nsub, sb = g0 - mt * S.nsub;
+      bool ok = true;
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
+        if (mt != cur) {
+          if (nload > 0 && !(ok = mbar_wait(a_empty, (nload - 1) & 1, err))) break;
+          mbar_arrive_expect_tx(a_full, SH::A_BYTES);
+          bulk_g2s(sA, Aw + (2 * mt + crank) * (int64_t)SH::A_BYTES, SH::A_BYTES, a_full);
+          cur = (int)mt;
+          ++nload;
+        }
+        const int st = it % kStages;
+        if (it >= kStages && !(ok = mbar_wait(b_empty + st, ((it / kStages) - 1) & 1, err))) break;
+        mbar_arrive_expect_tx(b_full + st, SH::BH_BYTES);
+        bulk_g2s(sB + st * SH::BH_BYTES, Bw + sb * (int64_t)(2 * SH::BH_BYTES) + crank * SH::BH_BYTES, SH::BH_BYTES,
+                 b_full + st);
+      }
+      if (!ok) {
+        atomicExch(err, 1);
+        if (nload > 0) mbar_wait(a_full, (nload - 1) & 1, err + 1);
+        for (int st = 0; st < kStages; ++st)
+          if (it > st) mbar_wait(b_full + st, ((it - 1 - st) / kStages) & 1, err + 1);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && crank == 1) {
+      // ---------------- relay (odd CTA): tell the even CTA's MMA thread ------
+      const uint32_t peer_a = cluster_addr(a_peer, 0);
+      int cur = -1, nload = 0, it = 0;
+      int64_t mt = g0 / S.nsub, sb = g0 - mt * S.nsub;
+      bool ok = true;
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
+        if (mt != cur) {
+          if (!(ok = mbar_wait(a_full, nload & 1, err))) break;
+          mbar_arrive_cluster(peer_a);
+          cur = (int)mt;
+          ++nload;
+        }
+        const int st = it % kStages;
+        if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+        mbar_arrive_cluster(cluster_addr(b_peer + st, 0));
+      }
+      if (!ok) atomicExch(err, 1);
+    } else if (lane == 0) {
+      // ---------------- MMA issuer (even CTA) --------------------------------
+      int cur = -1, nload = 0, it = 0;
+      bool ok = true;
+      const uint32_t id = idesc_i8_m256(8 * NS);
+      int64_t mt = g0 / S.nsub, sb = g0 - mt * S.nsub;
+      for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
+        if (mt != cur) {
+          if (nload > 0) mma_commit_pair(a_empty);  // both CTAs' A tiles are free once these MMAs finish
+          if (!(ok = mbar_wait(a_full, nload & 1, err))) break;
+          if (!(ok = mbar_wait(a_peer, nload & 1, err))) break;
+          fence_after();
+          cur = (int)mt;
+          ++nload;
+        }
+        const int st = it % kStages;
+        const int ab = it & 1;
+        if (it >= 2 && !(ok = mbar_wait(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
+        if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+        if (!(ok = mbar_wait(b_peer + st, (it / kStages) & 1, err))) break;
+        fence_after();
+        const uint8_t* bt = sB + st * SH::BH_BYTES;
+        const uint32_t dacc = tmem + ab * 256;
+        // Plane 0's first K step initialises blocks 0..7; blocks 8..14 were
+        // zeroed by the epilogue; every other MMA accumulates.
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int ks = 0; ks < KK / 32; ++ks)
+            mma_i8_pair(dacc + i * NS, smem_desc(sA + i * SH::TILE + ks * 256, SH::SBO),
+                        smem_desc(bt + ks * 256, SH::SBO), id, (i > 0 || ks > 0) ? 1u : 0u);
+        mma_commit_pair(b_empty + st);
+        mma_commit_pair(acc_full + ab);
+      }
+      if (!ok) atomicExch(err, 1);
+      mma_commit_pair(mma_done);
+      mbar_wait(mma_done, 0, err + 1);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (both CTAs): this CTA's 128 rows -------------
+    const int ew = warp - 2;
+    const int grp = ew >> 3;
+    const int quad = warp & 3;
+    const int half = (ew >> 2) & 1;
+    const int row = quad * 32 + lane;
+    const bool leader = (ew & 7) == 0 && lane == 0;
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + grp * 256 + half * 8;
+    uint64_t* cbuf = sC + grp * (128 * 16);
+    uint64_t* c_full = bars + 40 + grp;
+    const uint32_t release = crank == 0 ? 0u : cluster_addr(acc_empty + grp, 0);
+    const int64_t nsub = S.nsub;
+    int64_t g = g0 + grp;
+    int64_t mt = g / nsub, sb = g - mt * nsub;
+    auto advance = [&]() {
+      g += 2;
+      sb += 2;
+      while (sb >= nsub) {
+        sb -= nsub;
+        ++mt;
+      }
+    };
+    auto rowbase = [&]() { return (int32_t)(rbeg + mt * 256 + crank * 128); };
+    int loads = 0;
+    auto tma_load = [&]() {
+      mbar_arrive_expect_tx(c_full, 128 * 16 * 8);
+      tma_load_2d(cbuf, &cmap, (int32_t)(jend + sb * NS), rowbase(), c_full);
+      ++loads;
+    };
+    if (g < g1 && leader) tma_load();
+    bool ok = true;
+    for (int k = 0; g < g1; ++k) {
+      bool okw = __all_sync(0xffffffffu, mbar_wait(acc_full + grp, k & 1, err));
+      uint64_t x[8];
+      if (okw) {
+        fence_after();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          uint32_t a[15][4];
+#pragma unroll
+          for (int d = 0; d < 15; ++d) tmem_ld4(lane_base + d * NS + q * 4, a[d]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 4; ++c) x[4 * q + c] = m61_fold15(a, c);
+        }
+#pragma unroll
+        for (int d = 8; d < 15; ++d) tmem_st8_zero(lane_base + d * NS);
+        tmem_wait_st();
+        fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          if (crank == 0)
+            mbar_arrive(acc_empty + grp);
+          else
+            mbar_arrive_cluster(release);
+        }
+      }
+      if (okw) okw = __all_sync(0xffffffffu, mbar_wait(c_full, k & 1, err));
+      if (okw) {
+        uint64_t* rp = cbuf + row * 16;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint64_t* lp = rp + (half * 4 + q) * 2;
+          const uint32_t a = smem_u32(lp);
+          const int delta = (int)((a ^ (a >> 3)) & 0x70u) - (int)(a & 0x70u);
+          ulonglong2* pq = reinterpret_cast<ulonglong2*>(reinterpret_cast<uint8_t*>(lp) + delta);
+          const ulonglong2 v = *pq;
+          *pq = make_ulonglong2(m61_sub_lazy(v.x, x[2 * q]), m61_sub_lazy(v.y, x[2 * q + 1]));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      }
+      if (!group_bar_and(1 + grp, okw)) {
+        ok = false;
+        break;
+      }
+      if (leader) {
+        tma_store_2d(&cmap, (int32_t)(jend + sb * NS), rowbase(), cbuf);
+        bulk_commit();
+        bulk_wait_read0();
+      }
+      advance();
+      if (leader && g < g1) tma_load();
+    }
+    if (leader) {
+      bulk_wait_all0();
+      if (!ok && loads > 0) mbar_wait(c_full, (loads - 1) & 1, err + 1);
+    }
+    if (!ok) atomicExch(err, 1);
+  }
+  fence_before();
+  __syncthreads();
+  cluster_sync_all();  // no CTA leaves while its peer may still signal it or write its TMEM
+  fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 int limbs_for(uint64_t p) {
   const int bits = 64 - __builtin_clzll(p - 1);
   return bits <= 8 ? 1 : bits <= 16 ? 2 : bits <= 32 ? 4 : 8;
@@ -678,7 +959,9 @@ int limbs_for(uint64_t p) {
 
 template <int LIMBS, int KK>
 void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K, uint8_t* Aw, cudaStream_t st) {
-  const int mpad = ((rend - rbeg + 127) / 128) * 128;
+  // Padded to 256 rows (zero rows past rend), so CTA pairs find both of a
+  // 256-row tile's halves.
+  const int mpad = ((rend - rbeg + 255) / 256) * 256;
   const int64_t threads = (int64_t)mpad * Shape<LIMBS, KK>::KC;
   split_a_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(A, lda, r0, rbeg, rend, K, mpad, Aw);
 }
@@ -740,12 +1023,61 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
                                                                   err, cmap, use_tma);
 }
 
+// The pair kernel over 2^61 - 1 (C through TMA, so the caller checked the
+// alignment and made the tensor map): grid = 2 x the pairs that fit at once.
+template <int KK>
+cudaError_t update_pair_t(const uint8_t* Aw, const uint8_t* Bw, int rbeg, int rend, int jend, int cend, int max_ctas,
+                          int* err, const CUtensorMap& cmap, cudaStream_t st) {
+  using SH = PairShape<KK>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(trailing_tc_pair_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SH::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  Sched S;
+  S.mtiles = (rend - rbeg + 255) / 256;
+  S.nsub = (cend - jend + SH::NS - 1) / SH::NS;
+  const int64_t total = (int64_t)S.mtiles * S.nsub;
+  int pairs = max_ctas / 2;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = SH::SMEM;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  static int fit = 0;  // clusters of two that can be resident at once
+  if (!fit) {
+    cfg.gridDim = dim3(2 * pairs);
+    int c = 0;
+    if (cudaOccupancyMaxActiveClusters(&c, trailing_tc_pair_kernel<KK>, &cfg) != cudaSuccess || c < 1) {
+      cudaGetLastError();
+      c = 1;
+    }
+    fit = c;
+  }
+  if (pairs > fit) pairs = fit;
+  if (total < pairs) pairs = (int)total;
+  if (pairs < 1) pairs = 1;
+  cfg.gridDim = dim3(2 * pairs);
+  return cudaLaunchKernelEx(&cfg, trailing_tc_pair_kernel<KK>, Aw, Bw, (int32_t)rbeg, (int32_t)jend, S, err, cmap);
+}
+
 // (limb count, K tile) of a prime and an update depth.
 inline int limbs_of(uint64_t p) { return p == kM61 ? 8 : limbs_for(p); }
 
 }  // namespace tc
 
 int tc_crossover_n(uint64_t) { return 512; }
+
+// Whether updates over 2^61 - 1 may run on CTA pairs (modlin_set_tc_pairs).
+bool g_tc_pairs = true;
 
 // Calls OP(limbs, K tile) for fp.p and K, both compile-time constants.
 #define MODLIN_TC_DISPATCH(OP)                      \
@@ -788,6 +1120,12 @@ cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, 
   if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
   const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
   if (fp.p == kM61) {
+    // CTA pairs when C can move by TMA and there are rows for both halves.
+    CUtensorMap cmap;
+    if (g_tc_pairs && rend - rbeg > 128 && max_ctas >= 2 && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 &&
+        (jend & 1) == 0 && tc::make_c_map(&cmap, m, ld, rend, cend))
+      return K > 64 ? tc::update_pair_t<128>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st)
+                    : tc::update_pair_t<64>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st);
     if (K > 64)
       tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
     else

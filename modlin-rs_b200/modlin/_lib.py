@@ -105,6 +105,7 @@ def lib():
     _proto(L, "modlin_testing_grid_timeout_once", ci, [ctypes.c_longlong, ci])
     _proto(L, "modlin_plain_mac_peak", ci, [u64, ctypes.POINTER(ctypes.c_double)])
     _proto(L, "modlin_panel_pivots_device", ci, [u64, vp, szt, szt, szt, sztp, sztp, sztp, vp])
+    _proto(L, "modlin_set_tc_pairs", ci, [ci])
     _proto(L, "modlin_rank_prng_batch", ci, [u64, vp, szt, szt, ctypes.POINTER(RankOpts), sztp, PROGRESS, vp])
     _proto(L, "modlin_last_trailing_ms", ctypes.c_double, [])
     _proto(L, "modlin_last_trailing_macs", ctypes.c_double, [])
@@ -129,7 +130,7 @@ EXPORTED = [
     "modlin_field_mul", "modlin_rank", "modlin_rank_ex", "modlin_rank_device", "modlin_trailing_update_device",
     "modlin_linear_complexity", "modlin_linear_complexity_ex", "modlin_linear_complexity_device",
     "modlin_linear_complexity_device_noalloc", "modlin_testing_grid_timeout_once", "modlin_plain_mac_peak",
-    "modlin_panel_pivots_device", "modlin_rank_prng_batch",
+    "modlin_panel_pivots_device", "modlin_rank_prng_batch", "modlin_set_tc_pairs",
     "modlin_rank_batch", "modlin_rank_batch_device", "modlin_rank_batch_device_ex", "modlin_lc_batch", "modlin_lc_batch_device", "modlin_corank_prob",
     "modlin_corank_tail_pvalue", "modlin_lc_left_tail_pvalue", "modlin_pretty_p_value",
     "modlin_prng_new", "modlin_prng_name", "modlin_prng_fill", "modlin_prng_free", "modlin_prng_fill_device",

@@ -93,3 +93,26 @@ def test_two_panel_depth_large(M):
         two = run(M, p, run(M, p, C, L[:, :64], U[:64], "tc"), L[:, 64:], U[64:], "tc")
         assert np.array_equal(one, two)
         assert np.array_equal(two, run(M, p, run(M, p, C, L[:, :64], U[:64], "plain"), L[:, 64:], U[64:], "plain"))
+
+
+@pytest.mark.parametrize("K", [128, 64, 100, 17])
+def test_cta_pairs_equal_single_ctas(M, K):
+    """Updates over 2^61-1 on CTA pairs (M = 256 MMAs over two SMs, each
+    holding half of every B tile) equal the single-CTA kernel's and exact
+    Python integers, for row counts that leave the pair's second half partly
+    or wholly past the end."""
+    p = M61
+    L = M.lib()
+    rng = np.random.default_rng(K)
+    try:
+        for Mr, N in [(129, 16), (300, 130), (257, 64), (1000, 3000), (2048, 1536)]:
+            C, Lm, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
+            L.modlin_set_tc_pairs(1)
+            pair = run(M, p, C, Lm, U, "tc")
+            L.modlin_set_tc_pairs(0)
+            single = run(M, p, C, Lm, U, "tc")
+            assert np.array_equal(pair, single), (Mr, N, K)
+            if Mr * N <= 40000:
+                assert np.array_equal(pair, exact(p, C, Lm, U)), (Mr, N, K)
+    finally:
+        L.modlin_set_tc_pairs(1)
