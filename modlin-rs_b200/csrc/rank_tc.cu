@@ -804,13 +804,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
         if (mt != cur) {
-          if (!(ok = mbar_poll(a_full, nload & 1, err))) break;
+          if (!(ok = mbar_wait(a_full, nload & 1, err))) break;
           mbar_arrive_cluster(peer_a);
           cur = (int)mt;
           ++nload;
         }
         const int st = it % kStages;
-        if (!(ok = mbar_poll(b_full + st, (it / kStages) & 1, err))) break;
+        if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
         mbar_arrive_cluster(cluster_addr(b_peer + st, 0));
       }
       if (!ok) atomicExch(err, 1);
@@ -823,17 +823,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int64_t g = g0; g < g1 && ok; ++g, ++it, sb = sb + 1 == S.nsub ? (++mt, 0) : sb + 1) {
         if (mt != cur) {
           if (nload > 0) mma_commit_pair(a_empty);  // both CTAs' A tiles are free once these MMAs finish
-          if (!(ok = mbar_poll(a_full, nload & 1, err))) break;
-          if (!(ok = mbar_poll(a_peer, nload & 1, err))) break;
+          if (!(ok = mbar_wait(a_full, nload & 1, err))) break;
+          if (!(ok = mbar_wait(a_peer, nload & 1, err))) break;
           fence_after();
           cur = (int)mt;
           ++nload;
         }
         const int st = it % kStages;
         const int ab = it & 1;
-        if (it >= 2 && !(ok = mbar_poll(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
-        if (!(ok = mbar_poll(b_full + st, (it / kStages) & 1, err))) break;
-        if (!(ok = mbar_poll(b_peer + st, (it / kStages) & 1, err))) break;
+        if (it >= 2 && !(ok = mbar_wait(acc_empty + ab, ((it >> 1) - 1) & 1, err))) break;
+        if (!(ok = mbar_wait(b_full + st, (it / kStages) & 1, err))) break;
+        if (!(ok = mbar_wait(b_peer + st, (it / kStages) & 1, err))) break;
         fence_after();
         const uint8_t* bt = sB + st * SH::BH_BYTES;
         const uint32_t dacc = tmem + ab * 256;
@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (g < g1 && leader) tma_load();
     bool ok = true;
     for (int k = 0; g < g1; ++k) {
-      bool okw = warp_poll(acc_full + grp, k & 1, err);
+      bool okw = __all_sync(0xffffffffu, mbar_wait(acc_full + grp, k & 1, err));
       uint64_t x[8];
       if (okw) {
         fence_after();

@@ -67,14 +67,6 @@ __device__ __forceinline__ bool mbar_poll(uint64_t* bar, uint32_t parity, const 
   }
 }
 
-// A warp's wait on the critical path: lane 0 polls (no suspension, so it
-// sees the phase flip at once), the warp takes its answer.
-__device__ __forceinline__ bool warp_poll(uint64_t* bar, uint32_t parity, const int* err) {
-  bool ok = true;
-  if ((threadIdx.x & 31) == 0) ok = mbar_poll(bar, parity, err);
-  return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-}
-
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
