@@ -893,6 +893,8 @@ def main():
     ap.add_argument("--mode", default="replicas", choices=["replicas", "sharded"],
                     help="N > 1 GPUs: independent replicas of the rank (weak scaling, default) or one rank "
                          "with its column panels dealt over the GPUs (strong scaling, modlin.shard.rank_sharded)")
+    ap.add_argument("--tc-pairs", type=int, default=-1, choices=[-1, 0, 1],
+                    help="tensor-core updates over 2^61-1 on CTA pairs (1) or single CTAs (0); -1: library default")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="bm / rank-batch workloads: jobs in the batch (default: the full 65536 / 4096)")
     ap.add_argument("--workload", default="rank",
@@ -919,6 +921,8 @@ def main():
     import modlin
     from modlin import fp as mfp
 
+    if args.tc_pairs >= 0:
+        modlin.lib().modlin_set_tc_pairs(args.tc_pairs)
     # The AUTO choices measured on this GPU (a few seconds, before any timing).
     tune = (modlin.autotune()["choice"]
             if not args.no_autotune and args.workload not in ("trailing", "block-inverse", "fill") else None)
