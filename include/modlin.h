@@ -319,8 +319,8 @@ uint64_t modlin_kernel_launches(void);
  * counterpart: it is the denominator of the plain kernel's pipe fraction. */
 int modlin_plain_mac_peak(uint64_t p, double *modmac_per_s);
 /* Tensor-core updates over 2^61 - 1 run on CTA pairs (thread-block clusters
- * of two CTAs sharing each B tile, M = 256 MMAs) when enable = 1 (the
- * default) or on single CTAs when enable = 0; enable < 0 only queries.
+ * of two CTAs sharing each B tile, M = 256 MMAs) when enable = 1 or on single
+ * CTAs when enable = 0 (the default); enable < 0 only queries.
  * Returns the previous setting. Both kernels give the same, exact results;
  * no reference counterpart (a kernel choice, like MODLIN_RANK_TC). */
 int modlin_set_tc_pairs(int enable);

@@ -1076,8 +1076,9 @@ inline int limbs_of(uint64_t p) { return p == kM61 ? 8 : limbs_for(p); }
 
 int tc_crossover_n(uint64_t) { return 512; }
 
-// Whether updates over 2^61 - 1 may run on CTA pairs (modlin_set_tc_pairs).
-bool g_tc_pairs = true;
+// Whether updates over 2^61 - 1 run on CTA pairs (modlin_set_tc_pairs; off
+// by default: measured 1.5 % slower than single CTAs in the 16384^2 rank).
+bool g_tc_pairs = false;
 
 // Calls OP(limbs, K tile) for fp.p and K, both compile-time constants.
 #define MODLIN_TC_DISPATCH(OP)                      \

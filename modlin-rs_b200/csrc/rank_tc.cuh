@@ -34,7 +34,7 @@ cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, in
 cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
                       const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st);
 
-// Updates over 2^61 - 1 on CTA pairs (default) or on single CTAs.
+// Updates over 2^61 - 1 on CTA pairs or (default) on single CTAs.
 extern bool g_tc_pairs;
 
 }  // namespace modlin

@@ -104,6 +104,7 @@ def test_cta_pairs_equal_single_ctas(M, K):
     p = M61
     L = M.lib()
     rng = np.random.default_rng(K)
+    prev = L.modlin_set_tc_pairs(-1)
     try:
         for Mr, N in [(129, 16), (300, 130), (257, 64), (1000, 3000), (2048, 1536)]:
             C, Lm, U = rand_res(rng, p, (Mr, N)), rand_res(rng, p, (Mr, K)), rand_res(rng, p, (K, N))
@@ -115,4 +116,4 @@ def test_cta_pairs_equal_single_ctas(M, K):
             if Mr * N <= 40000:
                 assert np.array_equal(pair, exact(p, C, Lm, U)), (Mr, N, K)
     finally:
-        L.modlin_set_tc_pairs(1)
+        L.modlin_set_tc_pairs(prev)
