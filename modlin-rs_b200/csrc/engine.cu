@@ -277,31 +277,32 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   // Enqueue on `s` the four 64 x 64 blocks of the two-panel step at
   // (rr, cc) and copy the status word `slot` (nonzero: P11 or S singular)
   // to the host.
+  // The look-ahead chain of a two-panel step: six launches, each a kernel
+  // (programmatic dependent launches chain them without launch gaps).
   auto prep128 = [&](int rr, int cc, cudaStream_t s, int slot) -> cudaError_t {
-    cudaError_t e = cudaMemsetAsync(binv_status + slot, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
     const uint64_t* P11 = R.m + (int64_t)rr * ld + cc;
     const uint64_t* P12 = P11 + kPanel;
     const uint64_t* P21 = P11 + (int64_t)kPanel * ld;
     const uint64_t* P22 = P21 + kPanel;
-    launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, binv_status + slot, s);
-    launch_small_gemm64<F>(f, P21, ld, V11n, kPanel, nullptr, 0, Yb, kPanel, true, s);  // Y = P21 V11
-    launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s);      // S = P22 - Y P12
-    launch_small_gemm64<F>(f, V11n, kPanel, P12, ld, nullptr, 0, Zb, kPanel, true, s);  // Z = V11 P12
-    launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, binv_status + slot, s);
     // -P^-1 = [[-V11 - Z S^-1 Y, Z S^-1], [S^-1 Y, -S^-1]] (row stride 128):
     // TR = Z S^-1, BL = S^-1 Y, TL = -V11 - TR Y, BR = -S^-1.
     uint64_t* const TL = Pn;
     uint64_t* const TR = Pn + kPanel;
     uint64_t* const BL = Pn + 2 * blk;
     uint64_t* const BR = BL + kPanel;
-    launch_small_gemm64<F>(f, Zb, kPanel, VSn, kPanel, nullptr, 0, TR, 2 * kPanel, true, s);
-    launch_small_gemm64<F>(f, VSn, kPanel, Yb, kPanel, nullptr, 0, BL, 2 * kPanel, true, s);
+    launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, binv_status + slot, s, true);
+    const SgProb yz[2] = {{P21, V11n, nullptr, Yb, ld, kPanel, 0, kPanel, 1},    // Y = P21 V11
+                          {V11n, P12, nullptr, Zb, kPanel, ld, 0, kPanel, 1}};  // Z = V11 P12
+    launch_small_gemm64_batch<F>(f, yz, 2, s);
+    launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s);  // S = P22 - Y P12
+    launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, binv_status + slot, s);
+    const SgProb tb[3] = {{Zb, VSn, nullptr, TR, kPanel, kPanel, 0, 2 * kPanel, 1},
+                          {VSn, Yb, nullptr, BL, kPanel, kPanel, 0, 2 * kPanel, 1},
+                          {nullptr, nullptr, VSn, BR, 0, 0, kPanel, 2 * kPanel, 0}};
+    launch_small_gemm64_batch<F>(f, tb, 3, s);
     launch_small_gemm64<F>(f, TR, 2 * kPanel, Yb, kPanel, V11n, kPanel, TL, 2 * kPanel, true, s);
-    e = cudaMemcpy2DAsync(BR, 2 * kPanel * 8, VSn, kPanel * 8, kPanel * 8, kPanel, cudaMemcpyDeviceToDevice, s);
-    if (e != cudaSuccess) return e;
-    g_launches += 9;
-    e = cudaGetLastError();
+    g_launches += 6;
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(h_status + slot, binv_status + slot, sizeof(int), cudaMemcpyDeviceToHost, s);
   };
@@ -339,7 +340,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
         uint8_t* tB = C->tcB.as<uint8_t>();
         int* terr = C->tcerr.as<int>();
         if (rows > 0) {
-          CK(cudaMemsetAsync(Hb + (size_t)2 * kPanel * 2 * kPanel, 0, (size_t)rows * 2 * kPanel * 8, st));
+          launch_zero(Hb + (size_t)2 * kPanel * 2 * kPanel, (int64_t)rows * 2 * kPanel, st);
           const int64_t H0 = 2 * kPanel;  // H rows relative to r0, stride 128
           const uint64_t* X = R.m + (int64_t)r0 * ld + col;
           // H = X P^-1 = 0 - X (-P^-1), one K = 128 product.
@@ -404,9 +405,8 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       int status = pre_status;
       pre_status = -1;
       if (status < 0) {
-        CK(cudaMemsetAsync(binv_status, 0, sizeof(int), st));
-        launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st);
-        g_launches += 2;
+        launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st, true);
+        g_launches += 1;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h_status, binv_status, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -415,7 +415,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       if (status == 0) {
         const int rows = n - r0 - kPanel;
         if (rows > 0) {
-          CK(cudaMemsetAsync(Lbuf + (size_t)kPanel * kPanel, 0, (size_t)rows * kPanel * 8, st));
+          launch_zero(Lbuf + (size_t)kPanel * kPanel, (int64_t)rows * kPanel, st);
           // H (Lbuf rows 64 .. n - r0, relative to r0) = X_P * P^-1, as
           // 0 - X_P * (-P^-1).
           CK(launch_trailing_tc(*R.fp, Lbuf, kPanel, kPanel, n - r0, 0, kPanel, R.m + (int64_t)r0 * ld + col, ld, 0,
@@ -435,11 +435,10 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
                            C->tcBn.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
               CK(cudaEventRecord(C->ev_narrow, st));
               CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
-              CK(cudaMemsetAsync(binv_status + 1, 0, sizeof(int), C->aux));
-              launch_block_inverse<F>(f, R.m, ld, r0 + kPanel, jend, Vneg, binv_status + 1, C->aux);
+              launch_block_inverse<F>(f, R.m, ld, r0 + kPanel, jend, Vneg, binv_status + 1, C->aux, true);
               CK(cudaMemcpyAsync(h_status + 1, binv_status + 1, sizeof(int), cudaMemcpyDeviceToHost, C->aux));
               CK(cudaEventRecord(C->ev_inv, C->aux));
-              g_launches += 4;
+              g_launches += 3;
               cw = jend + kPanel;
             }
             if (cw < n) {
@@ -1589,11 +1588,10 @@ int modlin_block_inverse_device(uint64_t p, const uint64_t* d_P, size_t ldp, uin
   std::lock_guard<std::mutex> g_(C->mu);
   cudaStream_t st = user_stream(stream);
   CK(C->invst.ensure(sizeof(int)));
-  CK(cudaMemsetAsync(C->invst.p, 0, sizeof(int), st));
   if (p == kM61)
-    launch_block_inverse<FpM61>(FpM61(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st);
+    launch_block_inverse<FpM61>(FpM61(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st, true);
   else
-    launch_block_inverse<FpBarrett>(FpBarrett(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st);
+    launch_block_inverse<FpBarrett>(FpBarrett(fp), d_P, (int64_t)ldp, 0, 0, d_out, C->invst.as<int>(), st, true);
   g_launches++;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(C->h_out, C->invst.p, sizeof(int), cudaMemcpyDeviceToHost, st));

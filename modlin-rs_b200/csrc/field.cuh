@@ -149,6 +149,30 @@ struct FpM61 {
   MODLIN_HD uint64_t modulus() const { return kM61; }
 };
 
+// a^-1 mod 2^61 - 1 (a != 0) as a^(p-2), p - 2 = 2^61 - 3 = 4 (2^59 - 1) + 1.
+// With x_k = a^(2^k - 1), x_(j+k) = x_j^(2^k) x_k builds x_59 from x_1 in 58
+// squarings and 9 multiplications; then a^(p-2) = x_59^4 a. One dependent
+// chain of 70 modular multiplications: about half the single-thread latency
+// of the binary extended Euclid for this p.
+MODLIN_HD uint64_t m61_sqn(uint64_t x, int n) {
+  const FpM61 f;
+  for (int i = 0; i < n; ++i) x = f.mul(x, x);
+  return x;
+}
+MODLIN_HD uint64_t fp_inv_m61(uint64_t a) {
+  const FpM61 f;
+  const uint64_t x2 = f.mul(m61_sqn(a, 1), a);
+  const uint64_t x4 = f.mul(m61_sqn(x2, 2), x2);
+  const uint64_t x8 = f.mul(m61_sqn(x4, 4), x4);
+  const uint64_t x16 = f.mul(m61_sqn(x8, 8), x8);
+  const uint64_t x32 = f.mul(m61_sqn(x16, 16), x16);
+  const uint64_t x48 = f.mul(m61_sqn(x32, 16), x16);
+  const uint64_t x56 = f.mul(m61_sqn(x48, 8), x8);
+  const uint64_t x58 = f.mul(m61_sqn(x56, 2), x2);
+  const uint64_t x59 = f.mul(m61_sqn(x58, 1), a);
+  return f.mul(m61_sqn(x59, 2), a);
+}
+
 // src/fp.rs:97-113: Fermat inverse a^(p-2), a != 0.
 template <class F>
 MODLIN_HD uint64_t fp_pow(const F& f, uint64_t a, uint64_t e) {

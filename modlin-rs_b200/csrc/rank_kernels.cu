@@ -3,6 +3,7 @@
 // reference's src/fp.rs:125-255.
 #include <cuda_runtime.h>
 
+#include "launch.cuh"
 #include "rank_plain.cuh"
 #include "rank_kernels.cuh"
 #include "tc_ptx.cuh"
@@ -714,8 +715,11 @@ __device__ void rec_inverse(const F& f, uint64_t* X, int ldx, uint64_t* Out, int
 template <class F>
 __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
                                                                      int32_t r0, int32_t col,
-                                                                     uint64_t* __restrict__ Vneg, int* status, int rec) {
+                                                                     uint64_t* __restrict__ Vneg, int* status, int rec,
+                                                                     int reset_status) {
   extern __shared__ __align__(16) uint64_t smem_inv[];
+  pdl_wait();
+  if (reset_status && threadIdx.x == 0) *status = 0;
   if (rec) {
     __shared__ RecShared S;
     __shared__ uint64_t dl[5];  // level 64: d1, d2; level 32: d1, d2; the result's denominator
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
     rec_inverse<F, 64>(f, X, 64, Out, 64, &dl[4], scr, R, S, dl);
     if (!S.fail) {
       const uint64_t p = f.modulus();
-      if (threadIdx.x == 0) invd = fp_inv_binary(dl[4], p);
+      if (threadIdx.x == 0) invd = std::is_same<F, FpM61>::value ? fp_inv_m61(dl[4]) : fp_inv_binary(dl[4], p);
       __syncthreads();
       const uint64_t inv = invd;
       for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) {
@@ -747,24 +751,33 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 
 // ---------------------------------------------------------------------------
 // small_gemm64_kernel — C = D - A * B (negate) or C = D + A * B on 64 x 64
-// blocks mod p (D may be null: zero). 16 CTAs of 256 threads, one 16 x 16
-// output tile each (one output per thread, one reduction per output), so the
-// product spreads over the SMs a finished trailing update leaves free.
+// blocks mod p (D may be null: zero), or the copy C = D when A is null; up to
+// kSgMaxProbs independent problems per launch, 16 CTAs of 256 threads each,
+// one 16 x 16 output tile per CTA (one output per thread, one reduction per
+// output), so the products spread over the SMs a finished trailing update
+// leaves free.
 // ---------------------------------------------------------------------------
 constexpr int kSgTile = 16;
+struct SgBatch {
+  SgProb p[kSgMaxProbs];
+};
 template <class F>
-__global__ void __launch_bounds__(256) small_gemm64_kernel(F f, const uint64_t* __restrict__ A, int64_t lda,
-                                                            const uint64_t* __restrict__ B, int64_t ldb,
-                                                            const uint64_t* __restrict__ D, int64_t ldd,
-                                                            uint64_t* __restrict__ Cout, int64_t ldc, int negate) {
+__global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
   __shared__ uint64_t As[kSgTile][kPanel + 1], Bs[kPanel][kSgTile + 1];
+  pdl_wait();
+  const SgProb& P = batch.p[blockIdx.x >> 4];
   const int tid = threadIdx.x, i = tid >> 4, j = tid & 15;
-  const int ti = blockIdx.x >> 2, tj = blockIdx.x & 3;
+  const int ti = (blockIdx.x >> 2) & 3, tj = blockIdx.x & 3;
+  const int r = ti * kSgTile + i, c = tj * kSgTile + j;
+  if (!P.A) {  // copy
+    P.C[(int64_t)r * P.ldc + c] = P.D[(int64_t)r * P.ldd + c];
+    return;
+  }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int kk = j + 16 * q;
-    As[i][kk] = A[(int64_t)(ti * kSgTile + i) * lda + kk];
-    Bs[i + 16 * q][j] = B[(int64_t)(i + 16 * q) * ldb + tj * kSgTile + j];
+    As[i][kk] = P.A[(int64_t)(ti * kSgTile + i) * P.lda + kk];
+    Bs[i + 16 * q][j] = P.B[(int64_t)(i + 16 * q) * P.ldb + tj * kSgTile + j];
   }
   __syncthreads();
   const uint64_t p = f.modulus(), sb = f.safe_batch();
@@ -782,11 +795,16 @@ __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, const uint64_t* 
       }
     }
   }
-  const int r = ti * kSgTile + i, c = tj * kSgTile + j;
   uint64_t v = f.reduce(acc);
-  if (negate && v) v = p - v;
-  if (D) v = f.add(v, D[(int64_t)r * ldd + c]);
-  Cout[(int64_t)r * ldc + c] = v;
+  if (P.negate && v) v = p - v;
+  if (P.D) v = f.add(v, P.D[(int64_t)r * P.ldd + c]);
+  P.C[(int64_t)r * P.ldc + c] = v;
+}
+
+__global__ void zero_kernel(uint64_t* __restrict__ p, int64_t n) {
+  pdl_wait();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -860,7 +878,7 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int re
 
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
-                          cudaStream_t st) {
+                          cudaStream_t st, bool reset_status) {
   const size_t smem = kRecWords * sizeof(uint64_t);  // >= the pivoting path's kPanel * (kPanel + 1) words
   static bool attr_set = false;
   if (!attr_set) {
@@ -868,21 +886,38 @@ void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int
     attr_set = true;
   }
   const int rec = f.modulus() > (1ULL << 20);
-  block_inverse_kernel<F><<<1, kInvThreads, smem, st>>>(f, m, ld, r0, col, Vneg, status, rec);
+  launch_k(block_inverse_kernel<F>, dim3(1), dim3(kInvThreads), smem, st, 1, f, m, ld, (int32_t)r0, (int32_t)col,
+           Vneg, status, rec, reset_status ? 1 : 0);
+}
+
+template <class F>
+void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st) {
+  SgBatch b = {};
+  for (int i = 0; i < count && i < kSgMaxProbs; ++i) b.p[i] = probs[i];
+  const int n = count < kSgMaxProbs ? count : kSgMaxProbs;
+  launch_k(small_gemm64_kernel<F>, dim3(16 * n), dim3(256), 0, st, 1, f, b);
 }
 
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
                          int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st) {
-  small_gemm64_kernel<F><<<(kPanel / kSgTile) * (kPanel / kSgTile), 256, 0, st>>>(f, A, lda, B, ldb, D, ldd, C, ldc,
-                                                                                  negate ? 1 : 0);
+  const SgProb pr = {A, B, D, C, lda, ldb, ldd, ldc, negate ? 1 : 0};
+  launch_small_gemm64_batch<F>(f, &pr, 1, st);
+}
+
+void launch_zero(uint64_t* p, int64_t n, cudaStream_t st) {
+  if (n <= 0) return;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 1184) blocks = 1184;
+  launch_k(zero_kernel, dim3((unsigned)blocks), dim3(256), 0, st, 1, p, n);
 }
 
 #define INSTANTIATE(F)                                                                                          \
   template void launch_small_gemm64<F>(const F&, const uint64_t*, int64_t, const uint64_t*, int64_t,            \
                                        const uint64_t*, int64_t, uint64_t*, int64_t, bool, cudaStream_t);       \
   template void launch_block_inverse<F>(const F&, const uint64_t*, int64_t, int, int, uint64_t*, int*,          \
-                                        cudaStream_t);                                                          \
+                                        cudaStream_t, bool);                                                    \
+  template void launch_small_gemm64_batch<F>(const F&, const SgProb*, int, cudaStream_t);                       \
   template void launch_window<F>(const F&, const uint64_t*, int64_t, int, int, int, int, int, PanelState*,       \
                                  uint64_t*, uint64_t*, const uint64_t*, uint8_t*, cudaStream_t);                \
   template void launch_bulk<F>(const F&, uint64_t*, int64_t, int, int, int, int, int, PanelState*,              \

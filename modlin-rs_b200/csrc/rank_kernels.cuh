@@ -10,14 +10,32 @@
 namespace modlin {
 
 // Inverse of the 64 x 64 diagonal block (negated, row = panel column) or
-// *status = 1 when it is singular.
+// *status = 1 when it is singular. With reset_status the kernel first sets
+// *status = 0 (no separate memset in the stream).
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
-                          cudaStream_t st);
+                          cudaStream_t st, bool reset_status = false);
 // C = D - A * B (negate) or D + A * B on 64 x 64 blocks (D may be null).
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
                          int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st);
+// Up to kSgMaxProbs independent 64 x 64 products in one launch: problem i is
+// C = D - A * B (negate) or D + A * B (D may be null), or, with A null, the
+// copy C = D.
+struct SgProb {
+  const uint64_t* A;
+  const uint64_t* B;
+  const uint64_t* D;
+  uint64_t* C;
+  int64_t lda, ldb, ldd, ldc;
+  int negate;
+};
+constexpr int kSgMaxProbs = 3;
+template <class F>
+void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st);
+// n words at p set to zero (a kernel, so that it chains with programmatic
+// dependent launches).
+void launch_zero(uint64_t* p, int64_t n, cudaStream_t st);
 template <class F>
 void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
                    PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,

@@ -50,6 +50,7 @@
 
 #include "field.cuh"
 #include "rank_tc.cuh"
+#include "launch.cuh"
 #include "tc_ptx.cuh"
 
 namespace modlin {
@@ -98,6 +99,7 @@ template <int LIMBS, int KK>
 __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, int32_t r0, int32_t rbeg, int32_t rend,
                                int32_t K, int32_t mpad, uint8_t* __restrict__ Aw) {
   using SH = Shape<LIMBS, KK>;
+  pdl_wait();
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)mpad * SH::KC) return;
   const int ri_all = (int)(idx / SH::KC), kc = (int)(idx % SH::KC);
@@ -131,6 +133,7 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, i
 template <int LIMBS, int KK>
 __global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, int32_t jend, int32_t cend, int32_t K,
                                int32_t npad, uint8_t* __restrict__ Bw) {
+  pdl_wait();
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -227,6 +230,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* b_empty = bars + 8 + kStages;
   __shared__ uint32_t tmem_base_sh;
 
+  pdl_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(a_full, 1);
@@ -722,6 +726,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* b_peer = bars + 8 + 2 * kStages;  // even CTA: the odd CTA's B half has landed
   __shared__ uint32_t tmem_base_sh;
 
+  pdl_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t crank = cluster_rank();
   const int pair = blockIdx.x >> 1;
@@ -963,7 +968,8 @@ void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K
   // 256-row tile's halves.
   const int mpad = ((rend - rbeg + 255) / 256) * 256;
   const int64_t threads = (int64_t)mpad * Shape<LIMBS, KK>::KC;
-  split_a_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(A, lda, r0, rbeg, rend, K, mpad, Aw);
+  launch_k(split_a_kernel<LIMBS, KK>, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, 1, A, lda,
+           (int32_t)r0, (int32_t)rbeg, (int32_t)rend, (int32_t)K, (int32_t)mpad, Aw);
 }
 
 template <int LIMBS, int KK>
@@ -971,7 +977,8 @@ void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_
   constexpr int NS = Shape<LIMBS, KK>::NS;
   const int npad = ((cend - jend + NS - 1) / NS) * NS;
   const int64_t threads = (int64_t)npad * Shape<LIMBS, KK>::KC;
-  split_b_kernel<LIMBS, KK><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(B, ldb, jend, cend, K, npad, Bw);
+  launch_k(split_b_kernel<LIMBS, KK>, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, 1, B, ldb,
+           (int32_t)jend, (int32_t)cend, (int32_t)K, (int32_t)npad, Bw);
 }
 
 // Tensor map of C = m[0 .. rend) x [0 .. cend) (row stride ld) for 128 x 16
@@ -1019,8 +1026,8 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
   int use_tma = 0;
   if (std::is_same<F, FpM61>::value && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0)
     use_tma = make_c_map(&cmap, m, ld, rend, cend) ? 1 : 0;
-  trailing_tc_kernel<F, LIMBS, KK><<<grid, kThreads, smem, st>>>(f, Aw, Bw, m, ld, rbeg, rend, jend, cend, S, r64,
-                                                                  err, cmap, use_tma);
+  launch_k(trailing_tc_kernel<F, LIMBS, KK>, dim3(grid), dim3(kThreads), smem, st, 1, f, Aw, Bw, m, ld,
+           (int32_t)rbeg, (int32_t)rend, (int32_t)jend, (int32_t)cend, S, r64, err, cmap, use_tma);
 }
 
 // The pair kernel over 2^61 - 1 (C through TMA, so the caller checked the
@@ -1065,8 +1072,8 @@ cudaError_t update_pair_t(const uint8_t* Aw, const uint8_t* Bw, int rbeg, int re
   if (pairs > fit) pairs = fit;
   if (total < pairs) pairs = (int)total;
   if (pairs < 1) pairs = 1;
-  cfg.gridDim = dim3(2 * pairs);
-  return cudaLaunchKernelEx(&cfg, trailing_tc_pair_kernel<KK>, Aw, Bw, (int32_t)rbeg, (int32_t)jend, S, err, cmap);
+  return launch_k(trailing_tc_pair_kernel<KK>, dim3(2 * pairs), dim3(kThreads), SH::SMEM, st, 2, Aw, Bw,
+                  (int32_t)rbeg, (int32_t)jend, S, err, cmap);
 }
 
 // (limb count, K tile) of a prime and an update depth.
