@@ -93,9 +93,11 @@ struct Ctx {
   DevBuf tcA, tcB;  // limb planes for the tensor-core trailing update
   DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
   DevBuf binv;      // block-step status words and the negated block inverse
-  DevBuf tcBn;      // limb planes of the look-ahead (next panel) columns
+  DevBuf tcBn;      // limb planes of the narrow update's B operand (W = P^-1 U_next)
+  DevBuf tcBp;      // limb planes of -P^-1 (B operand of the multipliers H = X P^-1)
+  DevBuf tcX[2];    // limb planes of the block steps' X panels (alternating steps)
   cudaStream_t aux = nullptr;  // look-ahead stream: the next block's inverse
-  cudaEvent_t ev_narrow = nullptr, ev_inv = nullptr;
+  cudaEvent_t ev_narrow = nullptr, ev_inv[2] = {nullptr, nullptr};
   PanelState* h_ps = nullptr;
   int2* h_moves = nullptr;
   // linear-complexity workspaces
@@ -240,231 +242,226 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     return pr;
   };
 
-  // Block-step state: two status words (this panel, look-ahead), the
-  // negated block inverse, and the look-ahead result for the next panel
-  // (-1: none, 0: invertible, 1: singular).
-  int* binv_status = nullptr;
-  uint64_t* Vneg = nullptr;
-  int* h_status = reinterpret_cast<int*>(C->h_out);
-  int pre_status = -1;
-  // Two-panel steps (128 columns, K = 128 trailing update): blocks V11 = P11^-1
-  // (negated), Y = P21 V11, S = P22 - Y P12 and VS = S^-1 (negated), and the
-  // look-ahead result for the next two-panel step.
-  uint64_t *V11n = nullptr, *Yb = nullptr, *Sb = nullptr, *VSn = nullptr, *Zb = nullptr, *Pn = nullptr;
-  int pre128 = -1;
-  uint64_t* Hb = Lbuf;  // two-panel multipliers [H1 H2], row stride 128
+  // ---- Block pipeline (tensor-core path) -------------------------------
+  // A block step t takes w = 64 or 128 columns at (r0, c0): P = A[r0 ..
+  // r0+w, c0 .. c0+w) is the pivot block, X = A[r0+w .., c0 .. c0+w) the
+  // panel below it, U = A[r0 .. r0+w, c0+w ..) the pivot rows' trailing part.
+  // When P is invertible its rows and columns are this step's pivots (every
+  // panel column is independent of the earlier ones) and the trailing block
+  // becomes the Schur complement A - X P^-1 U, whose rank is the rank of what
+  // remains: the reference's panel elimination (src/fp.rs:146-248) in block
+  // form. Per step, on the main stream:
+  //   W = P^-1 U_next (the next step's wn columns; w x wn, 64 x 64 products),
+  //   narrow update A[r0+w .., next columns] -= X W (K = w),
+  //   H = X P^-1 (one n x w x w product), wide update A[.., rest] -= H U.
+  // On the second stream, after the narrow update, the chain of step t+1
+  // computes -P^-1 of the next block (one block inverse, or for w = 128 two
+  // inverses and six 64 x 64 products) while the wide update runs. The
+  // critical path per step is chain -> W -> narrow -> next chain; the
+  // multipliers H and the wide update are off it.
+  // The host queues step t before it knows whether step t's block is
+  // invertible: every kernel of step t carries Guard{gbad, t} and does
+  // nothing once a chain has recorded a failure at or before t. The host then
+  // reads step t's chain result (the GPU works on step t meanwhile); on a
+  // failure it waits for the skipped work, and the panel takes the general
+  // path below.
+  uint64_t* Hb = Lbuf;  // multipliers H, row stride w
   const size_t blk = (size_t)kPanel * kPanel;
+  uint64_t *V11n = nullptr, *Yb = nullptr, *Sb = nullptr, *VSn = nullptr, *Zb = nullptr;
+  uint64_t* Pn[2] = {nullptr, nullptr};  // -P^-1 of alternating steps (row stride w)
+  uint64_t* Wbuf = Ubuf;                 // W = P^-1 U_next: w rows, row stride n, absolute columns
+  int* gbad = nullptr;                   // first failed step of the pipeline (0x7f7f7f7f: none)
+  int* h_bad = reinterpret_cast<int*>(C->h_out) + 4;  // its value after each step's chain
+  uint8_t *tA = nullptr, *tB = nullptr, *tBn = nullptr, *tBp = nullptr, *tX[2] = {nullptr, nullptr};
+  int* terr = C->tcerr.as<int>();
   if (tc) {
-    CK(C->binv.ensure(256 + 10 * blk * 8));
+    CK(C->binv.ensure(256 + 14 * blk * 8));
     CK(C->lbuf.ensure((size_t)n * 2 * kPanel * 8));
+    CK(C->ubuf.ensure((size_t)2 * kPanel * n * 8));
+    CK(C->tcBn.ensure(tc_b_bytes(2 * kPanel)));
+    CK(C->tcBp.ensure(tc_b_bytes(2 * kPanel)));
+    CK(C->tcX[0].ensure(tc_a_bytes(n)));
+    CK(C->tcX[1].ensure(tc_a_bytes(n)));
     Lbuf = Hb = C->lbuf.as<uint64_t>();
-    V11n = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256) + blk;
+    Ubuf = Wbuf = C->ubuf.as<uint64_t>();
+    gbad = C->binv.as<int>() + 16;
+    V11n = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
     Yb = V11n + blk;
     Sb = Yb + blk;
     VSn = Sb + blk;
     Zb = VSn + blk;
-    Pn = Zb + blk;  // 128 x 128, row stride 128
-    CK(C->tcBn.ensure(tc_b_bytes(kPanel)));
-    binv_status = C->binv.as<int>();
-    Vneg = reinterpret_cast<uint64_t*>(C->binv.as<char>() + 256);
+    Pn[0] = Zb + blk;   // 128 x 128
+    Pn[1] = Pn[0] + 4 * blk;
+    tA = C->tcA.as<uint8_t>();
+    tB = C->tcB.as<uint8_t>();
+    tBn = C->tcBn.as<uint8_t>();
+    tBp = C->tcBp.as<uint8_t>();
+    tX[0] = C->tcX[0].as<uint8_t>();
+    tX[1] = C->tcX[1].as<uint8_t>();
     if (!C->aux) {
       CK(cudaStreamCreateWithFlags(&C->aux, cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&C->ev_narrow, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&C->ev_inv, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&C->ev_inv[0], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&C->ev_inv[1], cudaEventDisableTiming));
     }
   }
 
-  // Enqueue on `s` the four 64 x 64 blocks of the two-panel step at
-  // (rr, cc) and copy the status word `slot` (nonzero: P11 or S singular)
-  // to the host.
-  // The look-ahead chain of a two-panel step: six launches, each a kernel
-  // (programmatic dependent launches chain them without launch gaps).
-  auto prep128 = [&](int rr, int cc, cudaStream_t s, int slot) -> cudaError_t {
+  // -P^-1 of the 128 x 128 block at (rr, cc) into Pout (row stride 128) on
+  // `s`: P = [[P11, P12], [P21, P22]] in 64 x 64 blocks, V11 = P11^-1,
+  // S = P22 - P21 V11 P12, and
+  // -P^-1 = [[-V11 - Z S^-1 Y, Z S^-1], [S^-1 Y, -S^-1]] with Y = P21 V11,
+  // Z = V11 P12: six kernels (programmatic dependent launches chain them).
+  auto prep128 = [&](int rr, int cc, cudaStream_t s, uint64_t* Pout, const Guard& g) -> cudaError_t {
     const uint64_t* P11 = R.m + (int64_t)rr * ld + cc;
     const uint64_t* P12 = P11 + kPanel;
     const uint64_t* P21 = P11 + (int64_t)kPanel * ld;
     const uint64_t* P22 = P21 + kPanel;
-    // -P^-1 = [[-V11 - Z S^-1 Y, Z S^-1], [S^-1 Y, -S^-1]] (row stride 128):
-    // TR = Z S^-1, BL = S^-1 Y, TL = -V11 - TR Y, BR = -S^-1.
-    uint64_t* const TL = Pn;
-    uint64_t* const TR = Pn + kPanel;
-    uint64_t* const BL = Pn + 2 * blk;
+    uint64_t* const TL = Pout;
+    uint64_t* const TR = Pout + kPanel;
+    uint64_t* const BL = Pout + 2 * blk;
     uint64_t* const BR = BL + kPanel;
-    launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, binv_status + slot, s, true);
+    launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, nullptr, s, false, g);
     const SgProb yz[2] = {{P21, V11n, nullptr, Yb, ld, kPanel, 0, kPanel, 1},    // Y = P21 V11
                           {V11n, P12, nullptr, Zb, kPanel, ld, 0, kPanel, 1}};  // Z = V11 P12
-    launch_small_gemm64_batch<F>(f, yz, 2, s);
-    launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s);  // S = P22 - Y P12
-    launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, binv_status + slot, s);
-    const SgProb tb[3] = {{Zb, VSn, nullptr, TR, kPanel, kPanel, 0, 2 * kPanel, 1},
-                          {VSn, Yb, nullptr, BL, kPanel, kPanel, 0, 2 * kPanel, 1},
-                          {nullptr, nullptr, VSn, BR, 0, 0, kPanel, 2 * kPanel, 0}};
-    launch_small_gemm64_batch<F>(f, tb, 3, s);
-    launch_small_gemm64<F>(f, TR, 2 * kPanel, Yb, kPanel, V11n, kPanel, TL, 2 * kPanel, true, s);
+    launch_small_gemm64_batch<F>(f, yz, 2, s, g);
+    launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s, g);  // S = P22 - Y P12
+    launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, nullptr, s, false, g);
+    const SgProb tb[3] = {{Zb, VSn, nullptr, TR, kPanel, kPanel, 0, 2 * kPanel, 1},     // Z S^-1
+                          {VSn, Yb, nullptr, BL, kPanel, kPanel, 0, 2 * kPanel, 1},     // S^-1 Y
+                          {nullptr, nullptr, VSn, BR, 0, 0, kPanel, 2 * kPanel, 0}};   // -S^-1
+    launch_small_gemm64_batch<F>(f, tb, 3, s, g);
+    launch_small_gemm64<F>(f, TR, 2 * kPanel, Yb, kPanel, V11n, kPanel, TL, 2 * kPanel, true, s, g);
     g_launches += 6;
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyAsync(h_status + slot, binv_status + slot, sizeof(int), cudaMemcpyDeviceToHost, s);
+    return cudaGetLastError();
   };
+
+  // Chain of step t on the second stream: -P^-1 of the w x w block at (r, c)
+  // into Pn[t & 1]; a singular block records t in gbad. Its kernels are
+  // skipped once an earlier step has failed (Guard step t - 1). The host
+  // learns the result from h_bad[t & 1] after ev_inv[t & 1].
+  auto chain = [&](int t, int r, int c, int w) -> int {
+    const Guard gc{gbad, t - 1};
+    if (w == 2 * kPanel) {
+      CK(prep128(r, c, C->aux, Pn[t & 1], gc));
+    } else {
+      launch_block_inverse<F>(f, R.m, ld, r, c, Pn[t & 1], nullptr, C->aux, false, gc);
+      g_launches++;
+      CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(h_bad + (t & 1), gbad, sizeof(int), cudaMemcpyDeviceToHost, C->aux));
+    CK(cudaEventRecord(C->ev_inv[t & 1], C->aux));
+    return MODLIN_OK;
+  };
+
+  // W = P^-1 U[.., c1 .. c1+wn) = -(Pn U) into Wbuf (w rows, row stride n,
+  // columns c1 .. c1+wn), from 64 x 64 products accumulated over w / 64
+  // slices of the inner dimension.
+  auto make_w = [&](const uint64_t* Pt, int r0, int w, int c1, int wn, const Guard& g) -> int {
+    for (int kb = 0; kb < w / kPanel; ++kb) {
+      SgProb pr[4];
+      int np = 0;
+      for (int i = 0; i < w / kPanel; ++i)
+        for (int j = 0; j < wn / kPanel; ++j) {
+          uint64_t* Cw = Wbuf + (int64_t)i * kPanel * n + c1 + j * kPanel;
+          pr[np++] = {Pt + (int64_t)i * kPanel * w + kb * kPanel, R.m + (int64_t)(r0 + kb * kPanel) * ld + c1 + j * kPanel,
+                      kb ? Cw : nullptr, Cw, w, ld, n, n, 1};
+        }
+      launch_small_gemm64_batch<F>(f, pr, np, st, g);
+      g_launches++;
+    }
+    return cuda_rc(cudaGetLastError());
+  };
+
+  auto width = [&](int r, int c) -> int {
+    if (!tc) return 0;
+    if (n - r >= R.two_panel_min && n - c >= 2 * kPanel && n - r >= 2 * kPanel) return 2 * kPanel;
+    if (n - c >= kPanel && n - r >= kPanel) return kPanel;
+    return 0;
+  };
+
   double trailing_macs = 0;
+  // Block steps from (rank_io, col_io) while width() allows; returns with
+  // rank_io/col_io at the first panel they did not take and `failed` set
+  // when that panel's block was singular (it then takes the general path).
+  auto run_pipeline = [&](int& rank_io, int& col_io, bool& failed) -> int {
+    failed = false;
+    CK(cudaMemsetAsync(gbad, 0x7f, sizeof(int), st));  // no step has failed
+    CK(cudaEventRecord(C->ev_narrow, st));
+    CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
+    int t = 0, r0 = rank_io, c0 = col_io, w = width(r0, c0);
+    if (int rc = chain(0, r0, c0, w)) return rc;
+    CK(tc_split_a(*R.fp, R.m + c0, ld, 0, r0 + w, n, w, tX[0], st));
+    g_launches++;
+    for (;;) {
+      const int r1 = r0 + w, c1 = c0 + w;
+      const int wn = r1 < n ? width(r1, c1) : 0;  // the next step's width (0: none)
+      const int cw = c1 + wn;                      // first column of the wide update
+      const Guard g{gbad, t};
+      const uint64_t* Pt = Pn[t & 1];
+      CK(cudaStreamWaitEvent(st, C->ev_inv[t & 1], 0));
+      if (wn > 0) {
+        if (int rc = make_w(Pt, r0, w, c1, wn, g)) return rc;
+        CK(tc_split_b(*R.fp, Wbuf, n, c1, cw, w, tBn, st, g));
+        CK(tc_update(*R.fp, R.m, ld, r1, n, c1, cw, w, tX[t & 1], tBn, C->num_sms, terr, st, g));
+        CK(cudaEventRecord(C->ev_narrow, st));
+        CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
+        if (int rc = chain(t + 1, r1, c1, wn)) return rc;
+        CK(tc_split_a(*R.fp, R.m + c1, ld, 0, r1 + wn, n, wn, tX[(t + 1) & 1], st, g));
+        g_launches += 3;
+      }
+      if (r1 < n && cw < n) {
+        // H = X P^-1 = 0 - X (-P^-1) in Hb rows w .. n - r0 (relative to r0).
+        launch_zero(Hb + (size_t)w * w, (int64_t)(n - r1) * w, st, g);
+        CK(tc_split_b(*R.fp, Pt, w, 0, w, w, tBp, st, g));
+        // With a chain running, one SM stays free for it (a CTA waiting for
+        // that SM would hold up the whole product).
+        const int ctas = wn > 0 ? C->num_sms - 1 : C->num_sms;
+        CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g));
+        CK(tc_split_a(*R.fp, Hb, w, 0, w, n - r0, w, tA, st, g));
+        auto evp = take_events();
+        cudaEventRecord(evp.first, st);
+        CK(tc_split_b(*R.fp, R.m + (int64_t)r0 * ld, ld, cw, n, w, tB, st, g));
+        CK(tc_update(*R.fp, R.m, ld, r1, n, cw, n, w, tA, tB, ctas, terr, st, g));
+        cudaEventRecord(evp.second, st);
+        g_launches += 6;
+      }
+      // Step t's chain result (the GPU has step t queued meanwhile).
+      CK(cudaEventSynchronize(C->ev_inv[t & 1]));
+      if (h_bad[t & 1] <= t) {
+        // P_t is singular: nothing of step t (nor chain t + 1) took effect.
+        failed = true;
+        if (wn > 0) CK(cudaStreamWaitEvent(st, C->ev_inv[(t + 1) & 1], 0));
+        rank_io = r0;
+        col_io = c0;
+        return MODLIN_OK;
+      }
+      if (R.pcols)
+        for (int k = 0; k < w; ++k) R.pcols->push_back(c0 + k);
+      if (r1 < n && cw < n) trailing_macs += (double)(n - r1) * (n - cw) * w;
+      if (R.cb) R.cb(R.cb_ctx, (size_t)c1, (size_t)n);
+      if (wn == 0) {
+        rank_io = r1;
+        col_io = c1;
+        return MODLIN_OK;
+      }
+      r0 = r1;
+      c0 = c1;
+      w = wn;
+      ++t;
+    }
+  };
 
   int rank = 0, col = 0;
+  bool general_next = false;  // the panel at col had a singular block
   while (col < n && rank < n) {
+    if (!general_next && width(rank, col) > 0) {
+      if (int rc = run_pipeline(rank, col, general_next)) return rc;
+      continue;
+    }
+    general_next = false;
     const int jend = std::min(col + kPanel, n);
     const int W = jend - col;
     const int r0 = rank;
-    // Two-panel steps while the remaining block is at least two_panel_min
-    // rows (below that, one-panel steps have the shorter block chain).
-    if (tc && n - r0 >= R.two_panel_min && n - col >= 2 * kPanel && n - r0 >= 2 * kPanel) {
-      // Two-panel block step: P = A[r0 .. r0+128, col .. col+128) split into
-      // 64 x 64 blocks [P11 P12; P21 P22]. With V11 = P11^-1 and the Schur
-      // complement S = P22 - P21 V11 P12 invertible, P^-1 is assembled from
-      // 64 x 64 products on the look-ahead stream (prep128), the multipliers
-      // of the rows below come from one n x 128 x 128 product H = X_P P^-1,
-      // and the trailing block takes one K = 128 update
-      // A[r0+128.., col+128..] -= H * A[r0 .. r0+128, col+128..]: half the
-      // epilogue work per modMAC of two one-panel updates.
-      int status = pre128;
-      pre128 = -1;
-      if (status < 0) {
-        CK(prep128(r0, col, st, 0));
-        CK(cudaStreamSynchronize(st));
-        status = h_status[0];
-      }
-      if (status == 0) {
-        pre_status = -1;
-        const int c2 = col + 2 * kPanel;
-        const int rb = r0 + 2 * kPanel;
-        const int rows = n - rb;
-        uint8_t* tA = C->tcA.as<uint8_t>();
-        uint8_t* tB = C->tcB.as<uint8_t>();
-        int* terr = C->tcerr.as<int>();
-        if (rows > 0) {
-          launch_zero(Hb + (size_t)2 * kPanel * 2 * kPanel, (int64_t)rows * 2 * kPanel, st);
-          const int64_t H0 = 2 * kPanel;  // H rows relative to r0, stride 128
-          const uint64_t* X = R.m + (int64_t)r0 * ld + col;
-          // H = X P^-1 = 0 - X (-P^-1), one K = 128 product.
-          CK(launch_trailing_tc(*R.fp, Hb, H0, 2 * kPanel, n - r0, 0, 2 * kPanel, X, ld, 0, Pn, 2 * kPanel,
-                                2 * kPanel, tA, tB, C->num_sms, terr, st));
-          g_launches += 4;
-          if (c2 < n) {
-            const uint64_t* Ub = R.m + (int64_t)r0 * ld;  // the 128 pivot rows, as they are
-            auto evp = take_events();
-            cudaEventRecord(evp.first, st);
-            CK(tc_split_a(*R.fp, Hb, H0, r0, rb, n, 2 * kPanel, tA, st));
-            const bool ahead = c2 + 2 * kPanel <= n && n - rb >= 2 * kPanel && n - rb >= R.two_panel_min;
-            int cw = c2;
-            if (ahead) {
-              // The next step's 128 columns first; its blocks on the second
-              // stream while the rest updates.
-              CK(tc_split_b(*R.fp, Ub, ld, c2, c2 + 2 * kPanel, 2 * kPanel, C->tcBn.as<uint8_t>(), st));
-              CK(tc_update(*R.fp, R.m, ld, rb, n, c2, c2 + 2 * kPanel, 2 * kPanel, tA, C->tcBn.as<uint8_t>(),
-                           C->num_sms, terr, st));
-              CK(cudaEventRecord(C->ev_narrow, st));
-              CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
-              CK(prep128(rb, c2, C->aux, 1));
-              CK(cudaEventRecord(C->ev_inv, C->aux));
-              g_launches += 2;
-              cw = c2 + 2 * kPanel;
-            }
-            if (cw < n) {
-              CK(tc_split_b(*R.fp, Ub, ld, cw, n, 2 * kPanel, tB, st));
-              CK(tc_update(*R.fp, R.m, ld, rb, n, cw, n, 2 * kPanel, tA, tB, ahead ? C->num_sms - 1 : C->num_sms,
-                           terr, st));
-              g_launches += 2;
-            }
-            cudaEventRecord(evp.second, st);
-            g_launches += 1;
-            trailing_macs += (double)rows * (n - c2) * (2 * kPanel);
-            if (ahead) {
-              CK(cudaEventSynchronize(C->ev_inv));
-              pre128 = h_status[1];
-            }
-          }
-        }
-        if (R.pcols)
-          for (int k = 0; k < 2 * kPanel; ++k) R.pcols->push_back(col + k);
-        rank += 2 * kPanel;
-        col = c2;
-        if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
-        continue;
-      }
-    }
-    if (tc && W == kPanel && n - r0 >= kPanel) {
-      // Block step. When the diagonal block P = A[r0 .. r0+64, col .. jend) is
-      // invertible, its rows are this panel's pivot rows and col .. jend its
-      // pivot columns (every panel column is independent of the earlier
-      // ones); the rows below get the multipliers H = X_P * P^-1 and the
-      // trailing block becomes the Schur complement
-      // A[r0+64.., jend..] - H * A[r0 .. r0+64, jend..], whose rank is the
-      // rank of what remains — the same elimination as the reference's
-      // panel, with both products on the tensor cores and no row moves.
-      // Look-ahead: the next panel's 64 columns are updated first, and the
-      // next block's inverse runs on a second stream (on the SM the wide
-      // update leaves free) while the rest of the trailing block updates.
-      int status = pre_status;
-      pre_status = -1;
-      if (status < 0) {
-        launch_block_inverse<F>(f, R.m, ld, r0, col, Vneg, binv_status, st, true);
-        g_launches += 1;
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(h_status, binv_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        status = h_status[0];
-      }
-      if (status == 0) {
-        const int rows = n - r0 - kPanel;
-        if (rows > 0) {
-          launch_zero(Lbuf + (size_t)kPanel * kPanel, (int64_t)rows * kPanel, st);
-          // H (Lbuf rows 64 .. n - r0, relative to r0) = X_P * P^-1, as
-          // 0 - X_P * (-P^-1).
-          CK(launch_trailing_tc(*R.fp, Lbuf, kPanel, kPanel, n - r0, 0, kPanel, R.m + (int64_t)r0 * ld + col, ld, 0,
-                                Vneg, kPanel, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(), C->num_sms,
-                                C->tcerr.as<int>(), st));
-          g_launches += 4;
-          if (jend < n) {
-            const uint64_t* Ub = R.m + (int64_t)r0 * ld;  // the pivot rows
-            auto evp = take_events();
-            cudaEventRecord(evp.first, st);
-            CK(tc_split_a(*R.fp, Lbuf, kPanel, r0, r0 + kPanel, n, kPanel, C->tcA.as<uint8_t>(), st));
-            const bool ahead = jend + kPanel <= n && n - (r0 + kPanel) >= kPanel;
-            int cw = jend;
-            if (ahead) {
-              CK(tc_split_b(*R.fp, Ub, ld, jend, jend + kPanel, kPanel, C->tcBn.as<uint8_t>(), st));
-              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, jend, jend + kPanel, kPanel, C->tcA.as<uint8_t>(),
-                           C->tcBn.as<uint8_t>(), C->num_sms, C->tcerr.as<int>(), st));
-              CK(cudaEventRecord(C->ev_narrow, st));
-              CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
-              launch_block_inverse<F>(f, R.m, ld, r0 + kPanel, jend, Vneg, binv_status + 1, C->aux, true);
-              CK(cudaMemcpyAsync(h_status + 1, binv_status + 1, sizeof(int), cudaMemcpyDeviceToHost, C->aux));
-              CK(cudaEventRecord(C->ev_inv, C->aux));
-              g_launches += 3;
-              cw = jend + kPanel;
-            }
-            if (cw < n) {
-              CK(tc_split_b(*R.fp, Ub, ld, cw, n, kPanel, C->tcB.as<uint8_t>(), st));
-              // One SM left to the look-ahead inverse.
-              CK(tc_update(*R.fp, R.m, ld, r0 + kPanel, n, cw, n, kPanel, C->tcA.as<uint8_t>(), C->tcB.as<uint8_t>(),
-                           ahead ? C->num_sms - 1 : C->num_sms, C->tcerr.as<int>(), st));
-              g_launches += 2;
-            }
-            cudaEventRecord(evp.second, st);
-            g_launches += 1;
-            trailing_macs += (double)rows * (n - jend) * kPanel;
-            if (ahead) {
-              CK(cudaEventSynchronize(C->ev_inv));
-              pre_status = h_status[1];
-            }
-          }
-        }
-        if (R.pcols)
-          for (int k = 0; k < kPanel; ++k) R.pcols->push_back(col + k);
-        rank += kPanel;
-        col = jend;
-        if (R.cb) R.cb(R.cb_ctx, (size_t)col, (size_t)n);
-        continue;
-      }
-    }
     CK(cudaMemsetAsync(ps, 0, sizeof(PanelState), st));
     g_launches++;
     int round = 0, pb_lo = 0;

@@ -22,6 +22,21 @@ namespace modlin {
 
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Predication of a speculatively queued block step. The rank driver queues
+// step t of its block pipeline before it knows whether step t's diagonal
+// block is invertible; the look-ahead chain that inverts it records the
+// first failed step in a device word (*bad = min(*bad, t)), and every kernel
+// of step t is launched with Guard{bad, t} and does nothing when
+// *bad <= step. The word only changes between launches that depend on each
+// other (a chain and the kernels of its own or a later step), so every
+// thread of a launch reads the same value. A default Guard never skips.
+struct Guard {
+  int* bad = nullptr;
+  int step = 0;
+};
+
+__device__ __forceinline__ bool guard_skip(const Guard& g) { return g.bad && __ldcg(g.bad) <= g.step; }
+
 // PDL is on unless the environment sets MODLIN_PDL=0 (read once).
 inline bool pdl_enabled() {
   static const bool on = [] {

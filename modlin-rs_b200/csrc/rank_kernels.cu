@@ -452,7 +452,7 @@ int plain_blocks_per_sm() {
 // ---------------------------------------------------------------------------
 template <class F>
 __device__ void gj64_inverse(const F& f, const uint64_t* __restrict__ m, int64_t ld, int32_t r0, int32_t col,
-                             uint64_t* __restrict__ Vneg, int* status, uint64_t* smem_inv) {
+                             uint64_t* __restrict__ Vneg, int* status, const Guard& g, uint64_t* smem_inv) {
   uint64_t(*M)[kPanel + 1] = reinterpret_cast<uint64_t(*)[kPanel + 1]>(smem_inv);
   __shared__ uint64_t d[kPanel], dinv[kPanel], sc[kPanel];
   __shared__ int32_t pc[kPanel];
@@ -483,7 +483,10 @@ __device__ void gj64_inverse(const F& f, const uint64_t* __restrict__ m, int64_t
     const bool hi = !((used >> (lane + 32)) & 1) && nz[c & 1][lane + 32];
     const uint32_t b0 = __ballot_sync(0xffffffffu, lo), b1 = __ballot_sync(0xffffffffu, hi);
     if ((b0 | b1) == 0) {  // no pivot in column c: P is singular
-      if (tid == 0) *status = 1;
+      if (tid == 0) {
+        if (status) *status = 1;
+        if (g.bad) atomicMin(g.bad, g.step + 1);  // the chain of step g.step + 1 failed
+      }
       return;
     }
     const int piv = b0 ? __ffs(b0) - 1 : 31 + __ffs(b1);
@@ -716,10 +719,11 @@ template <class F>
 __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const uint64_t* __restrict__ m, int64_t ld,
                                                                      int32_t r0, int32_t col,
                                                                      uint64_t* __restrict__ Vneg, int* status, int rec,
-                                                                     int reset_status) {
+                                                                     int reset_status, Guard g) {
   extern __shared__ __align__(16) uint64_t smem_inv[];
   pdl_wait();
-  if (reset_status && threadIdx.x == 0) *status = 0;
+  if (guard_skip(g)) return;  // an earlier step of the pipeline failed
+  if (reset_status && status && threadIdx.x == 0) *status = 0;
   if (rec) {
     __shared__ RecShared S;
     __shared__ uint64_t dl[5];  // level 64: d1, d2; level 32: d1, d2; the result's denominator
@@ -746,7 +750,7 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
     }
     __syncthreads();
   }
-  gj64_inverse(f, m, ld, r0, col, Vneg, status, smem_inv);
+  gj64_inverse(f, m, ld, r0, col, Vneg, status, g, smem_inv);
 }
 
 // ---------------------------------------------------------------------------
@@ -760,11 +764,13 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(F f, const u
 constexpr int kSgTile = 16;
 struct SgBatch {
   SgProb p[kSgMaxProbs];
+  Guard g;
 };
 template <class F>
 __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
   __shared__ uint64_t As[kSgTile][kPanel + 1], Bs[kPanel][kSgTile + 1];
   pdl_wait();
+  if (guard_skip(batch.g)) return;
   const SgProb& P = batch.p[blockIdx.x >> 4];
   const int tid = threadIdx.x, i = tid >> 4, j = tid & 15;
   const int ti = (blockIdx.x >> 2) & 3, tj = blockIdx.x & 3;
@@ -801,8 +807,9 @@ __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
   P.C[(int64_t)r * P.ldc + c] = v;
 }
 
-__global__ void zero_kernel(uint64_t* __restrict__ p, int64_t n) {
+__global__ void zero_kernel(uint64_t* __restrict__ p, int64_t n, Guard g) {
   pdl_wait();
+  if (guard_skip(g)) return;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = 0;
 }
@@ -878,7 +885,7 @@ void launch_trailing_plain(const F& f, uint64_t* m, int64_t ld, int rbeg, int re
 
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
-                          cudaStream_t st, bool reset_status) {
+                          cudaStream_t st, bool reset_status, const Guard& g) {
   const size_t smem = kRecWords * sizeof(uint64_t);  // >= the pivoting path's kPanel * (kPanel + 1) words
   static bool attr_set = false;
   if (!attr_set) {
@@ -887,12 +894,13 @@ void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int
   }
   const int rec = f.modulus() > (1ULL << 20);
   launch_k(block_inverse_kernel<F>, dim3(1), dim3(kInvThreads), smem, st, 1, f, m, ld, (int32_t)r0, (int32_t)col,
-           Vneg, status, rec, reset_status ? 1 : 0);
+           Vneg, status, rec, reset_status ? 1 : 0, g);
 }
 
 template <class F>
-void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st) {
+void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st, const Guard& g) {
   SgBatch b = {};
+  b.g = g;
   for (int i = 0; i < count && i < kSgMaxProbs; ++i) b.p[i] = probs[i];
   const int n = count < kSgMaxProbs ? count : kSgMaxProbs;
   launch_k(small_gemm64_kernel<F>, dim3(16 * n), dim3(256), 0, st, 1, f, b);
@@ -900,24 +908,25 @@ void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaS
 
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
-                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st) {
+                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st, const Guard& g) {
   const SgProb pr = {A, B, D, C, lda, ldb, ldd, ldc, negate ? 1 : 0};
-  launch_small_gemm64_batch<F>(f, &pr, 1, st);
+  launch_small_gemm64_batch<F>(f, &pr, 1, st, g);
 }
 
-void launch_zero(uint64_t* p, int64_t n, cudaStream_t st) {
+void launch_zero(uint64_t* p, int64_t n, cudaStream_t st, const Guard& g) {
   if (n <= 0) return;
   int64_t blocks = (n + 255) / 256;
   if (blocks > 1184) blocks = 1184;
-  launch_k(zero_kernel, dim3((unsigned)blocks), dim3(256), 0, st, 1, p, n);
+  launch_k(zero_kernel, dim3((unsigned)blocks), dim3(256), 0, st, 1, p, n, g);
 }
 
 #define INSTANTIATE(F)                                                                                          \
   template void launch_small_gemm64<F>(const F&, const uint64_t*, int64_t, const uint64_t*, int64_t,            \
-                                       const uint64_t*, int64_t, uint64_t*, int64_t, bool, cudaStream_t);       \
+                                       const uint64_t*, int64_t, uint64_t*, int64_t, bool, cudaStream_t,        \
+                                       const Guard&);                                                           \
   template void launch_block_inverse<F>(const F&, const uint64_t*, int64_t, int, int, uint64_t*, int*,          \
-                                        cudaStream_t, bool);                                                    \
-  template void launch_small_gemm64_batch<F>(const F&, const SgProb*, int, cudaStream_t);                       \
+                                        cudaStream_t, bool, const Guard&);                                      \
+  template void launch_small_gemm64_batch<F>(const F&, const SgProb*, int, cudaStream_t, const Guard&);         \
   template void launch_window<F>(const F&, const uint64_t*, int64_t, int, int, int, int, int, PanelState*,       \
                                  uint64_t*, uint64_t*, const uint64_t*, uint8_t*, cudaStream_t);                \
   template void launch_bulk<F>(const F&, uint64_t*, int64_t, int, int, int, int, int, PanelState*,              \

@@ -5,20 +5,24 @@
 #include <cstdint>
 
 #include "field.cuh"
+#include "launch.cuh"
 #include "rank_plain.cuh"
 
 namespace modlin {
 
-// Inverse of the 64 x 64 diagonal block (negated, row = panel column) or
-// *status = 1 when it is singular. With reset_status the kernel first sets
-// *status = 0 (no separate memset in the stream).
+// Inverse of the 64 x 64 diagonal block (negated, row = panel column) or,
+// when it is singular, *status = 1 (status may be null) and, with a guard,
+// *g.bad = min(*g.bad, g.step + 1): the inverse belongs to the look-ahead
+// chain of step g.step + 1 and does nothing once step g.step has failed.
+// With reset_status the kernel first sets *status = 0 (no separate memset).
 template <class F>
 void launch_block_inverse(const F& f, const uint64_t* m, int64_t ld, int r0, int col, uint64_t* Vneg, int* status,
-                          cudaStream_t st, bool reset_status = false);
+                          cudaStream_t st, bool reset_status = false, const Guard& g = Guard());
 // C = D - A * B (negate) or D + A * B on 64 x 64 blocks (D may be null).
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
-                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st);
+                         int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st,
+                         const Guard& g = Guard());
 // Up to kSgMaxProbs independent 64 x 64 products in one launch: problem i is
 // C = D - A * B (negate) or D + A * B (D may be null), or, with A null, the
 // copy C = D.
@@ -30,12 +34,13 @@ struct SgProb {
   int64_t lda, ldb, ldd, ldc;
   int negate;
 };
-constexpr int kSgMaxProbs = 3;
+constexpr int kSgMaxProbs = 4;
 template <class F>
-void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st);
+void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaStream_t st,
+                               const Guard& g = Guard());
 // n words at p set to zero (a kernel, so that it chains with programmatic
 // dependent launches).
-void launch_zero(uint64_t* p, int64_t n, cudaStream_t st);
+void launch_zero(uint64_t* p, int64_t n, cudaStream_t st, const Guard& g = Guard());
 template <class F>
 void launch_window(const F& f, const uint64_t* m, int64_t ld, int n, int r0, int col, int W, int round,
                    PanelState* ps, uint64_t* Upanel, uint64_t* G, const uint64_t* Lbuf, uint8_t* is_pivot,

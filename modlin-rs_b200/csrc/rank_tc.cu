@@ -97,9 +97,10 @@ struct Sched {
 // ---------------------------------------------------------------------------
 template <int LIMBS, int KK>
 __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, int32_t r0, int32_t rbeg, int32_t rend,
-                               int32_t K, int32_t mpad, uint8_t* __restrict__ Aw) {
+                               int32_t K, int32_t mpad, uint8_t* __restrict__ Aw, Guard g) {
   using SH = Shape<LIMBS, KK>;
   pdl_wait();
+  if (guard_skip(g)) return;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)mpad * SH::KC) return;
   const int ri_all = (int)(idx / SH::KC), kc = (int)(idx % SH::KC);
@@ -132,8 +133,9 @@ __global__ void split_a_kernel(const uint64_t* __restrict__ Lbuf, int64_t lda, i
 // ---------------------------------------------------------------------------
 template <int LIMBS, int KK>
 __global__ void split_b_kernel(const uint64_t* __restrict__ Ubuf, int64_t ldU, int32_t jend, int32_t cend, int32_t K,
-                               int32_t npad, uint8_t* __restrict__ Bw) {
+                               int32_t npad, uint8_t* __restrict__ Bw, Guard g) {
   pdl_wait();
+  if (guard_skip(g)) return;
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,7 +210,7 @@ template <class F, int LIMBS, int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
                        int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err,
-                       const __grid_constant__ CUtensorMap cmap, int use_tma) {
+                       const __grid_constant__ CUtensorMap cmap, int use_tma, Guard guard) {
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
   // p = 2^61 - 1: two epilogue groups of 8 warps, one per accumulator buffer.
@@ -229,8 +231,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* b_full = bars + 8;
   uint64_t* b_empty = bars + 8 + kStages;
   __shared__ uint32_t tmem_base_sh;
+  __shared__ int skip_sh;
 
   pdl_wait();
+  if (threadIdx.x == 0) skip_sh = guard_skip(guard);
+  __syncthreads();
+  if (skip_sh) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(a_full, 1);
@@ -706,7 +712,8 @@ struct PairShape {
 template <int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_pair_kernel(const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, int32_t rbeg,
-                            int32_t jend, Sched S, int* err, const __grid_constant__ CUtensorMap cmap) {
+                            int32_t jend, Sched S, int* err, const __grid_constant__ CUtensorMap cmap,
+                            Guard guard) {
   using SH = PairShape<KK>;
   constexpr int NS = SH::NS;
   constexpr int kStages = SH::STAGES;
@@ -725,8 +732,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* b_empty = bars + 8 + kStages;
   uint64_t* b_peer = bars + 8 + 2 * kStages;  // even CTA: the odd CTA's B half has landed
   __shared__ uint32_t tmem_base_sh;
+  __shared__ int skip_sh;
 
   pdl_wait();
+  // Both CTAs of a pair read the same word (it cannot change during the launch).
+  if (threadIdx.x == 0) skip_sh = guard_skip(guard);
+  __syncthreads();
+  if (skip_sh) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t crank = cluster_rank();
   const int pair = blockIdx.x >> 1;
@@ -963,22 +975,24 @@ int limbs_for(uint64_t p) {
 }
 
 template <int LIMBS, int KK>
-void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K, uint8_t* Aw, cudaStream_t st) {
+void split_a_t(const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K, uint8_t* Aw, cudaStream_t st,
+               const Guard& g) {
   // Padded to 256 rows (zero rows past rend), so CTA pairs find both of a
   // 256-row tile's halves.
   const int mpad = ((rend - rbeg + 255) / 256) * 256;
   const int64_t threads = (int64_t)mpad * Shape<LIMBS, KK>::KC;
   launch_k(split_a_kernel<LIMBS, KK>, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, 1, A, lda,
-           (int32_t)r0, (int32_t)rbeg, (int32_t)rend, (int32_t)K, (int32_t)mpad, Aw);
+           (int32_t)r0, (int32_t)rbeg, (int32_t)rend, (int32_t)K, (int32_t)mpad, Aw, g);
 }
 
 template <int LIMBS, int KK>
-void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw, cudaStream_t st) {
+void split_b_t(const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw, cudaStream_t st,
+               const Guard& g) {
   constexpr int NS = Shape<LIMBS, KK>::NS;
   const int npad = ((cend - jend + NS - 1) / NS) * NS;
   const int64_t threads = (int64_t)npad * Shape<LIMBS, KK>::KC;
   launch_k(split_b_kernel<LIMBS, KK>, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, st, 1, B, ldb,
-           (int32_t)jend, (int32_t)cend, (int32_t)K, (int32_t)npad, Bw);
+           (int32_t)jend, (int32_t)cend, (int32_t)K, (int32_t)npad, Bw, g);
 }
 
 // Tensor map of C = m[0 .. rend) x [0 .. cend) (row stride ld) for 128 x 16
@@ -1007,7 +1021,7 @@ static bool make_c_map(CUtensorMap* map, uint64_t* m, int64_t ld, int rend, int 
 
 template <class F, int LIMBS, int KK>
 void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint8_t* Aw,
-              const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st) {
+              const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st, const Guard& g) {
   using SH = Shape<LIMBS, KK>;
   Sched S;
   S.mtiles = (rend - rbeg + 127) / 128;
@@ -1027,14 +1041,14 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
   if (std::is_same<F, FpM61>::value && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0)
     use_tma = make_c_map(&cmap, m, ld, rend, cend) ? 1 : 0;
   launch_k(trailing_tc_kernel<F, LIMBS, KK>, dim3(grid), dim3(kThreads), smem, st, 1, f, Aw, Bw, m, ld,
-           (int32_t)rbeg, (int32_t)rend, (int32_t)jend, (int32_t)cend, S, r64, err, cmap, use_tma);
+           (int32_t)rbeg, (int32_t)rend, (int32_t)jend, (int32_t)cend, S, r64, err, cmap, use_tma, g);
 }
 
 // The pair kernel over 2^61 - 1 (C through TMA, so the caller checked the
 // alignment and made the tensor map): grid = 2 x the pairs that fit at once.
 template <int KK>
 cudaError_t update_pair_t(const uint8_t* Aw, const uint8_t* Bw, int rbeg, int rend, int jend, int cend, int max_ctas,
-                          int* err, const CUtensorMap& cmap, cudaStream_t st) {
+                          int* err, const CUtensorMap& cmap, cudaStream_t st, const Guard& g) {
   using SH = PairShape<KK>;
   static bool attr = false;
   if (!attr) {
@@ -1073,7 +1087,7 @@ cudaError_t update_pair_t(const uint8_t* Aw, const uint8_t* Bw, int rbeg, int re
   if (total < pairs) pairs = (int)total;
   if (pairs < 1) pairs = 1;
   return launch_k(trailing_tc_pair_kernel<KK>, dim3(2 * pairs), dim3(kThreads), SH::SMEM, st, 2, Aw, Bw,
-                  (int32_t)rbeg, (int32_t)jend, S, err, cmap);
+                  (int32_t)rbeg, (int32_t)jend, S, err, cmap, g);
 }
 
 // (limb count, K tile) of a prime and an update depth.
@@ -1103,27 +1117,28 @@ size_t tc_a_bytes(int rows) { return (size_t)((rows + 127) / 128 + 1) * 128 * tc
 size_t tc_b_bytes(int cols) { return (size_t)((cols + 127) / 128 + 1) * 128 * tc::kKMax * 8; }
 
 cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
-                       uint8_t* Aw, cudaStream_t st) {
+                       uint8_t* Aw, cudaStream_t st, const Guard& g) {
   if (rbeg >= rend) return cudaSuccess;
   if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
-#define MODLIN_SPLIT_A(LL, KK) tc::split_a_t<LL, KK>(A, lda, r0, rbeg, rend, K, Aw, st)
+#define MODLIN_SPLIT_A(LL, KK) tc::split_a_t<LL, KK>(A, lda, r0, rbeg, rend, K, Aw, st, g)
   MODLIN_TC_DISPATCH(MODLIN_SPLIT_A);
 #undef MODLIN_SPLIT_A
   return cudaGetLastError();
 }
 
 cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
-                       cudaStream_t st) {
+                       cudaStream_t st, const Guard& g) {
   if (jend >= cend) return cudaSuccess;
   if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
-#define MODLIN_SPLIT_B(LL, KK) tc::split_b_t<LL, KK>(B, ldb, jend, cend, K, Bw, st)
+#define MODLIN_SPLIT_B(LL, KK) tc::split_b_t<LL, KK>(B, ldb, jend, cend, K, Bw, st, g)
   MODLIN_TC_DISPATCH(MODLIN_SPLIT_B);
 #undef MODLIN_SPLIT_B
   return cudaGetLastError();
 }
 
 cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
-                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st) {
+                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st,
+                      const Guard& g) {
   if (rbeg >= rend || jend >= cend) return cudaSuccess;
   if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
   const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
@@ -1132,17 +1147,17 @@ cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, 
     CUtensorMap cmap;
     if (g_tc_pairs && rend - rbeg > 128 && max_ctas >= 2 && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 &&
         (jend & 1) == 0 && tc::make_c_map(&cmap, m, ld, rend, cend))
-      return K > 64 ? tc::update_pair_t<128>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st)
-                    : tc::update_pair_t<64>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st);
+      return K > 64 ? tc::update_pair_t<128>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st, g)
+                    : tc::update_pair_t<64>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st, g);
     if (K > 64)
-      tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
+      tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g);
     else
-      tc::update_t<FpM61, 8, 64>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st);
+      tc::update_t<FpM61, 8, 64>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g);
     return cudaGetLastError();
   }
   const FpBarrett f(fp);
 #define MODLIN_UPDATE(LL, KK) \
-  tc::update_t<FpBarrett, LL, KK>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st)
+  tc::update_t<FpBarrett, LL, KK>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g)
   MODLIN_TC_DISPATCH(MODLIN_UPDATE);
 #undef MODLIN_UPDATE
   return cudaGetLastError();
@@ -1150,12 +1165,12 @@ cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, 
 
 cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
                                const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
-                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st) {
+                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st, const Guard& g) {
   if (rbeg >= rend || jend >= cend || K <= 0) return cudaSuccess;
   if (K > tc::kKMax) return cudaErrorInvalidValue;
-  cudaError_t e = tc_split_a(fp, Lbuf, lda, r0, rbeg, rend, K, Aw, st);
-  if (e == cudaSuccess) e = tc_split_b(fp, Ubuf, ldU, jend, cend, K, Bw, st);
-  if (e == cudaSuccess) e = tc_update(fp, m, ld, rbeg, rend, jend, cend, K, Aw, Bw, num_sms, err, st);
+  cudaError_t e = tc_split_a(fp, Lbuf, lda, r0, rbeg, rend, K, Aw, st, g);
+  if (e == cudaSuccess) e = tc_split_b(fp, Ubuf, ldU, jend, cend, K, Bw, st, g);
+  if (e == cudaSuccess) e = tc_update(fp, m, ld, rbeg, rend, jend, cend, K, Aw, Bw, num_sms, err, st, g);
   return e;
 }
 

@@ -6,6 +6,7 @@
 #include <cstdint>
 
 #include "field.cuh"
+#include "launch.cuh"
 
 namespace modlin {
 
@@ -20,7 +21,8 @@ size_t tc_b_bytes(int cols);
 // bounded wait inside the kernel expired.
 cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend,
                                const uint64_t* Lbuf, int64_t lda, int r0, const uint64_t* Ubuf, int64_t ldU, int K,
-                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st);
+                               uint8_t* Aw, uint8_t* Bw, int num_sms, int* err, cudaStream_t st,
+                               const Guard& g = Guard());
 
 // The three steps of launch_trailing_tc, for callers that reuse one operand's
 // limb planes across launches: limb planes of A rows [rbeg, rend) (row r at
@@ -28,11 +30,15 @@ cudaError_t launch_trailing_tc(const FieldParams& fp, uint64_t* m, int64_t ld, i
 // update A[rbeg..rend, jend..cend] -= A * B on at most max_ctas SMs. The same
 // K (<= 64 or <= 128: two plane layouts) must be given to all three.
 cudaError_t tc_split_a(const FieldParams& fp, const uint64_t* A, int64_t lda, int r0, int rbeg, int rend, int K,
-                       uint8_t* Aw, cudaStream_t st);
+                       uint8_t* Aw, cudaStream_t st, const Guard& g = Guard());
 cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, int jend, int cend, int K, uint8_t* Bw,
-                       cudaStream_t st);
+                       cudaStream_t st, const Guard& g = Guard());
 cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
-                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st);
+                      const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st,
+                      const Guard& g = Guard());
+
+// Each launch takes an optional Guard (launch.cuh): a predicated block step
+// whose kernels do nothing once the step is known to have failed.
 
 // Updates over 2^61 - 1 on CTA pairs or (default) on single CTAs.
 extern bool g_tc_pairs;
