@@ -372,6 +372,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     return cuda_rc(cudaGetLastError());
   };
 
+  const bool fused = tc && tc_limb_out_supported(R.fp->p);  // limb planes from the epilogues
   auto width = [&](int r, int c) -> int {
     if (!tc) return 0;
     if (n - r >= R.two_panel_min && n - c >= 2 * kPanel && n - r >= 2 * kPanel) return 2 * kPanel;
@@ -402,28 +403,44 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       if (wn > 0) {
         if (int rc = make_w(Pt, r0, w, c1, wn, g)) return rc;
         CK(tc_split_b(*R.fp, Wbuf, n, c1, cw, w, tBn, st, g));
-        CK(tc_update(*R.fp, R.m, ld, r1, n, c1, cw, w, tX[t & 1], tBn, C->num_sms, terr, st, g));
+        // Over 2^61 - 1 the narrow update also writes the next step's X
+        // (its rows from r1 + wn) as limb planes.
+        LimbOut lx;
+        if (fused) lx = LimbOut{tX[(t + 1) & 1], r1 + wn, wn > kPanel ? 2 * kPanel : kPanel, 0};
+        CK(tc_update(*R.fp, R.m, ld, r1, n, c1, cw, w, tX[t & 1], tBn, C->num_sms, terr, st, g, lx));
         CK(cudaEventRecord(C->ev_narrow, st));
         CK(cudaStreamWaitEvent(C->aux, C->ev_narrow, 0));
         if (int rc = chain(t + 1, r1, c1, wn)) return rc;
-        CK(tc_split_a(*R.fp, R.m + c1, ld, 0, r1 + wn, n, wn, tX[(t + 1) & 1], st, g));
-        g_launches += 3;
+        if (!fused) {
+          CK(tc_split_a(*R.fp, R.m + c1, ld, 0, r1 + wn, n, wn, tX[(t + 1) & 1], st, g));
+          g_launches++;
+        }
+        g_launches += 2;
       }
       if (r1 < n && cw < n) {
-        // H = X P^-1 = 0 - X (-P^-1) in Hb rows w .. n - r0 (relative to r0).
-        launch_zero(Hb + (size_t)w * w, (int64_t)(n - r1) * w, st, g);
+        // H = X P^-1 = 0 - X (-P^-1) for the rows r1 .. n (relative rows
+        // w .. n - r0), as the wide update's A operand. Over 2^61 - 1 the
+        // product writes H's limb planes directly; otherwise H goes through
+        // Hb and a split.
         CK(tc_split_b(*R.fp, Pt, w, 0, w, w, tBp, st, g));
         // With a chain running, one SM stays free for it (a CTA waiting for
         // that SM would hold up the whole product).
         const int ctas = wn > 0 ? C->num_sms - 1 : C->num_sms;
-        CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g));
-        CK(tc_split_a(*R.fp, Hb, w, 0, w, n - r0, w, tA, st, g));
+        if (fused) {
+          const LimbOut lh{tA, w, w > kPanel ? 2 * kPanel : kPanel, 1};
+          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g, lh));
+        } else {
+          launch_zero(Hb + (size_t)w * w, (int64_t)(n - r1) * w, st, g);
+          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g));
+          CK(tc_split_a(*R.fp, Hb, w, 0, w, n - r0, w, tA, st, g));
+          g_launches += 2;
+        }
         auto evp = take_events();
         cudaEventRecord(evp.first, st);
         CK(tc_split_b(*R.fp, R.m + (int64_t)r0 * ld, ld, cw, n, w, tB, st, g));
         CK(tc_update(*R.fp, R.m, ld, r1, n, cw, n, w, tA, tB, ctas, terr, st, g));
         cudaEventRecord(evp.second, st);
-        g_launches += 6;
+        g_launches += 4;
       }
       // Step t's chain result (the GPU has step t queued meanwhile).
       CK(cudaEventSynchronize(C->ev_inv[t & 1]));

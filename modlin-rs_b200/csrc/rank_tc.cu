@@ -206,11 +206,51 @@ __device__ __forceinline__ uint64_t m61_sub_lazy(uint64_t cv, uint64_t x) {
   return y1 >= kM61 ? y1 - kM61 : y1;
 }
 
+// In place 8 x 8 byte transpose: afterwards byte c of t[i] is the former
+// byte i of t[c] (swap the off-diagonal 4 x 4, then 2 x 2, then 1 x 1
+// blocks).
+__device__ __forceinline__ void bytes_transpose8(uint64_t (&t)[8]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint64_t x = ((t[j] >> 32) ^ t[j + 4]) & 0x00000000FFFFFFFFull;
+    t[j] ^= x << 32;
+    t[j + 4] ^= x;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j += (j & 1) ? 3 : 1) {  // 0, 1, 4, 5
+    const uint64_t x = ((t[j] >> 16) ^ t[j + 2]) & 0x0000FFFF0000FFFFull;
+    t[j] ^= x << 16;
+    t[j + 2] ^= x;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j += 2) {
+    const uint64_t x = ((t[j] >> 8) ^ t[j + 1]) & 0x00FF00FF00FF00FFull;
+    t[j] ^= x << 8;
+    t[j + 1] ^= x;
+  }
+}
+
+// Writes the 8 residues v (columns kcol .. kcol+7 of K, kcol a multiple of
+// 8, of limb row lr) as bytes of the 8 limb planes in the A-operand layout
+// of a K = kk update (split_a_kernel's layout).
+__device__ __forceinline__ void store_limbs8(uint8_t* Aw, int kk, int64_t lr, int kcol, const uint64_t (&v)[8]) {
+  uint64_t t[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) t[c] = v[c];
+  bytes_transpose8(t);
+  const int64_t tile = 128 * (int64_t)kk;
+  const int lmt = (int)(lr >> 7), lri = (int)(lr & 127);
+  uint8_t* base = Aw + (int64_t)lmt * 8 * tile + (((lri >> 3) * (kk >> 4) + (kcol >> 4)) * 8 + (lri & 7)) * 16 +
+                  (kcol & 15);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) *reinterpret_cast<uint64_t*>(base + i * tile) = t[i];
+}
+
 template <class F, int LIMBS, int KK>
 __global__ void __launch_bounds__(kThreads, 1)
     trailing_tc_kernel(F f, const uint8_t* __restrict__ Aw, const uint8_t* __restrict__ Bw, uint64_t* m, int64_t ld,
                        int32_t rbeg, int32_t rend, int32_t jend, int32_t cend, Sched S, uint64_t r64, int* err,
-                       const __grid_constant__ CUtensorMap cmap, int use_tma, Guard guard) {
+                       const __grid_constant__ CUtensorMap cmap, int use_tma, Guard guard, LimbOut lo) {
   using SH = Shape<LIMBS, KK>;
   constexpr int NS = SH::NS;
   // p = 2^61 - 1: two epilogue groups of 8 warps, one per accumulator buffer.
@@ -399,8 +439,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int c = 0; c < 8; ++c) cv[c] = (r < rend && c0 + c < cend) ? __ldcs(src + c) : 0;
     };
+    // lo.c_zero: C is zero and not written (only the limb planes are).
+    const bool czero = lo.c_zero != 0;
+    const bool tma = use_tma && !czero;
+    auto put_limbs = [&](uint64_t (&res)[8]) {
+      const int64_t r = (int64_t)rbeg + mt * 128 + row;
+      const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
+      const int64_t lr = r - lo.row0;
+      if (r >= rend || lr < 0) return;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c0 + c >= cend) res[c] = 0;
+      store_limbs8(lo.Aw, lo.kk, lr, (int)(c0 - jend), res);
+    };
     uint64_t cv[8];
-    if (g < g1) {
+    if (g < g1 && !czero) {
       if (!use_tma)
         load_c(cv);
       else if (leader)
@@ -425,7 +478,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(acc_empty + grp);
       }
-      if (use_tma) {
+      uint64_t res[8];
+      if (tma) {
         if (okw) okw = __all_sync(0xffffffffu, mbar_wait(c_full, k & 1, err));
         if (okw) {
           // Row `row`, 16-byte chunks 4 half .. +4 of the 128-byte row; the
@@ -439,7 +493,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int delta = (int)((a ^ (a >> 3)) & 0x70u) - (int)(a & 0x70u);
             ulonglong2* pq = reinterpret_cast<ulonglong2*>(reinterpret_cast<uint8_t*>(lp) + delta);
             const ulonglong2 v = *pq;
-            *pq = make_ulonglong2(m61_sub_lazy(v.x, x[2 * q]), m61_sub_lazy(v.y, x[2 * q + 1]));
+            res[2 * q] = m61_sub_lazy(v.x, x[2 * q]);
+            res[2 * q + 1] = m61_sub_lazy(v.y, x[2 * q + 1]);
+            *pq = make_ulonglong2(res[2 * q], res[2 * q + 1]);
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         }
@@ -454,6 +510,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           bulk_commit();
           bulk_wait_read0();  // the buffer is read; it can take the next tile
         }
+        if (lo.Aw) put_limbs(res);
         advance();
         if (leader && g < g1) tma_load();
       } else {
@@ -463,17 +520,20 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const int64_t r = (int64_t)rbeg + mt * 128 + row;
         const int64_t c0 = (int64_t)jend + sb * NS + half * 8;
-        uint64_t* dst = m + r * ld + c0;
-        if (r < rend) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) res[c] = m61_sub_lazy(czero ? 0 : cv[c], x[c]);
+        if (!czero && r < rend) {
+          uint64_t* dst = m + r * ld + c0;
 #pragma unroll
           for (int c = 0; c < 8; ++c)
-            if (c0 + c < cend) dst[c] = m61_sub_lazy(cv[c], x[c]);
+            if (c0 + c < cend) dst[c] = res[c];
         }
+        if (lo.Aw) put_limbs(res);
         advance();
-        if (g < g1) load_c(cv);
+        if (g < g1 && !czero) load_c(cv);
       }
     }
-    if (leader && use_tma) {
+    if (leader && tma) {
       bulk_wait_all0();  // stores complete
       if (!ok && loads > 0) mbar_wait(c_full, (loads - 1) & 1, err + 1);  // a load still landing
     }
@@ -1021,7 +1081,8 @@ static bool make_c_map(CUtensorMap* map, uint64_t* m, int64_t ld, int rend, int 
 
 template <class F, int LIMBS, int KK>
 void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, const uint8_t* Aw,
-              const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st, const Guard& g) {
+              const uint8_t* Bw, int max_ctas, uint64_t r64, int* err, cudaStream_t st, const Guard& g,
+              const LimbOut& lo) {
   using SH = Shape<LIMBS, KK>;
   Sched S;
   S.mtiles = (rend - rbeg + 127) / 128;
@@ -1038,10 +1099,10 @@ void update_t(const F& f, uint64_t* m, int64_t ld, int rbeg, int rend, int jend,
   CUtensorMap cmap;
   std::memset(&cmap, 0, sizeof cmap);
   int use_tma = 0;
-  if (std::is_same<F, FpM61>::value && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0)
+  if (std::is_same<F, FpM61>::value && !lo.c_zero && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 && (jend & 1) == 0)
     use_tma = make_c_map(&cmap, m, ld, rend, cend) ? 1 : 0;
   launch_k(trailing_tc_kernel<F, LIMBS, KK>, dim3(grid), dim3(kThreads), smem, st, 1, f, Aw, Bw, m, ld,
-           (int32_t)rbeg, (int32_t)rend, (int32_t)jend, (int32_t)cend, S, r64, err, cmap, use_tma, g);
+           (int32_t)rbeg, (int32_t)rend, (int32_t)jend, (int32_t)cend, S, r64, err, cmap, use_tma, g, lo);
 }
 
 // The pair kernel over 2^61 - 1 (C through TMA, so the caller checked the
@@ -1138,26 +1199,27 @@ cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, in
 
 cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
                       const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st,
-                      const Guard& g) {
+                      const Guard& g, const LimbOut& lo) {
   if (rbeg >= rend || jend >= cend) return cudaSuccess;
+  if (lo.Aw && (fp.p != kM61 || (lo.kk != 64 && lo.kk != 128))) return cudaErrorInvalidValue;
   if (K <= 0 || K > tc::kKMax) return cudaErrorInvalidValue;
   const uint64_t r64 = (uint64_t)(((u128)1 << 64) % fp.p);
   if (fp.p == kM61) {
     // CTA pairs when C can move by TMA and there are rows for both halves.
     CUtensorMap cmap;
-    if (g_tc_pairs && rend - rbeg > 128 && max_ctas >= 2 && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 &&
+    if (g_tc_pairs && !lo.Aw && rend - rbeg > 128 && max_ctas >= 2 && (ld & 1) == 0 && ((uintptr_t)m & 15) == 0 &&
         (jend & 1) == 0 && tc::make_c_map(&cmap, m, ld, rend, cend))
       return K > 64 ? tc::update_pair_t<128>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st, g)
                     : tc::update_pair_t<64>(Aw, Bw, rbeg, rend, jend, cend, max_ctas, err, cmap, st, g);
     if (K > 64)
-      tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g);
+      tc::update_t<FpM61, 8, 128>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g, lo);
     else
-      tc::update_t<FpM61, 8, 64>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g);
+      tc::update_t<FpM61, 8, 64>(FpM61(fp), m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g, lo);
     return cudaGetLastError();
   }
   const FpBarrett f(fp);
 #define MODLIN_UPDATE(LL, KK) \
-  tc::update_t<FpBarrett, LL, KK>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g)
+  tc::update_t<FpBarrett, LL, KK>(f, m, ld, rbeg, rend, jend, cend, Aw, Bw, max_ctas, r64, err, st, g, lo)
   MODLIN_TC_DISPATCH(MODLIN_UPDATE);
 #undef MODLIN_UPDATE
   return cudaGetLastError();

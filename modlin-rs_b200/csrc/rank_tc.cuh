@@ -10,6 +10,18 @@
 
 namespace modlin {
 
+// Extra output of a tensor-core update over 2^61 - 1: the result rows from
+// row0 on are also written as limb planes in the A-operand layout of a
+// K = kk update (the layout tc_split_a writes for rows row0 ..), so the next
+// product needs no split kernel. With c_zero the update computes 0 - A * B:
+// C is neither read nor written (only the limb planes are).
+struct LimbOut {
+  uint8_t* Aw = nullptr;
+  int32_t row0 = 0;
+  int32_t kk = 64;
+  int32_t c_zero = 0;
+};
+
 // Smallest side for which MODLIN_RANK_AUTO uses the tensor-core update.
 int tc_crossover_n(uint64_t p);
 // Workspace bytes for the limb planes of L (rows x K) and U (K x cols), K <= 128.
@@ -35,7 +47,9 @@ cudaError_t tc_split_b(const FieldParams& fp, const uint64_t* B, int64_t ldb, in
                        cudaStream_t st, const Guard& g = Guard());
 cudaError_t tc_update(const FieldParams& fp, uint64_t* m, int64_t ld, int rbeg, int rend, int jend, int cend, int K,
                       const uint8_t* Aw, const uint8_t* Bw, int max_ctas, int* err, cudaStream_t st,
-                      const Guard& g = Guard());
+                      const Guard& g = Guard(), const LimbOut& lo = LimbOut());
+// Whether tc_update takes a LimbOut for this prime (2^61 - 1 only).
+inline bool tc_limb_out_supported(uint64_t p) { return p == kM61; }
 
 // Each launch takes an optional Guard (launch.cuh): a predicated block step
 // whose kernels do nothing once the step is known to have failed.
