@@ -94,7 +94,7 @@ struct Ctx {
   DevBuf tcerr;     // bounded-wait error words of the tensor-core kernel
   DevBuf binv;      // block-step status words and the negated block inverse
   DevBuf tcBn;      // limb planes of the narrow update's B operand (W = P^-1 U_next)
-  DevBuf tcBp;      // limb planes of -P^-1 (B operand of the multipliers H = X P^-1)
+  DevBuf tcBp[2];   // limb planes of -P^-1 (B operand of the multipliers H = X P^-1), alternating steps
   DevBuf tcX[2];    // limb planes of the block steps' X panels (alternating steps)
   cudaStream_t aux = nullptr;  // look-ahead stream: the next block's inverse
   cudaEvent_t ev_narrow = nullptr, ev_inv[2] = {nullptr, nullptr};
@@ -272,14 +272,15 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   uint64_t* Wbuf = Ubuf;                 // W = P^-1 U_next: w rows, row stride n, absolute columns
   int* gbad = nullptr;                   // first failed step of the pipeline (0x7f7f7f7f: none)
   int* h_bad = reinterpret_cast<int*>(C->h_out) + 4;  // its value after each step's chain
-  uint8_t *tA = nullptr, *tB = nullptr, *tBn = nullptr, *tBp = nullptr, *tX[2] = {nullptr, nullptr};
+  uint8_t *tA = nullptr, *tB = nullptr, *tBn = nullptr, *tBp[2] = {nullptr, nullptr}, *tX[2] = {nullptr, nullptr};
   int* terr = C->tcerr.as<int>();
   if (tc) {
     CK(C->binv.ensure(256 + 14 * blk * 8));
     CK(C->lbuf.ensure((size_t)n * 2 * kPanel * 8));
     CK(C->ubuf.ensure((size_t)2 * kPanel * n * 8));
     CK(C->tcBn.ensure(tc_b_bytes(2 * kPanel)));
-    CK(C->tcBp.ensure(tc_b_bytes(2 * kPanel)));
+    CK(C->tcBp[0].ensure(tc_b_bytes(2 * kPanel)));
+    CK(C->tcBp[1].ensure(tc_b_bytes(2 * kPanel)));
     CK(C->tcX[0].ensure(tc_a_bytes(n)));
     CK(C->tcX[1].ensure(tc_a_bytes(n)));
     Lbuf = Hb = C->lbuf.as<uint64_t>();
@@ -295,7 +296,8 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     tA = C->tcA.as<uint8_t>();
     tB = C->tcB.as<uint8_t>();
     tBn = C->tcBn.as<uint8_t>();
-    tBp = C->tcBp.as<uint8_t>();
+    tBp[0] = C->tcBp[0].as<uint8_t>();
+    tBp[1] = C->tcBp[1].as<uint8_t>();
     tX[0] = C->tcX[0].as<uint8_t>();
     tX[1] = C->tcX[1].as<uint8_t>();
     if (!C->aux) {
@@ -321,14 +323,14 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
     uint64_t* const BL = Pout + 2 * blk;
     uint64_t* const BR = BL + kPanel;
     launch_block_inverse<F>(f, R.m, ld, rr, cc, V11n, nullptr, s, false, g);
-    const SgProb yz[2] = {{P21, V11n, nullptr, Yb, ld, kPanel, 0, kPanel, 1},    // Y = P21 V11
-                          {V11n, P12, nullptr, Zb, kPanel, ld, 0, kPanel, 1}};  // Z = V11 P12
+    const SgProb yz[2] = {{P21, V11n, nullptr, Yb, ld, kPanel, 0, kPanel, 1, kPanel},    // Y = P21 V11
+                          {V11n, P12, nullptr, Zb, kPanel, ld, 0, kPanel, 1, kPanel}};  // Z = V11 P12
     launch_small_gemm64_batch<F>(f, yz, 2, s, g);
     launch_small_gemm64<F>(f, Yb, kPanel, P12, ld, P22, ld, Sb, kPanel, true, s, g);  // S = P22 - Y P12
     launch_block_inverse<F>(f, Sb, kPanel, 0, 0, VSn, nullptr, s, false, g);
-    const SgProb tb[3] = {{Zb, VSn, nullptr, TR, kPanel, kPanel, 0, 2 * kPanel, 1},     // Z S^-1
-                          {VSn, Yb, nullptr, BL, kPanel, kPanel, 0, 2 * kPanel, 1},     // S^-1 Y
-                          {nullptr, nullptr, VSn, BR, 0, 0, kPanel, 2 * kPanel, 0}};   // -S^-1
+    const SgProb tb[3] = {{Zb, VSn, nullptr, TR, kPanel, kPanel, 0, 2 * kPanel, 1, kPanel},     // Z S^-1
+                          {VSn, Yb, nullptr, BL, kPanel, kPanel, 0, 2 * kPanel, 1, kPanel},     // S^-1 Y
+                          {nullptr, nullptr, VSn, BR, 0, 0, kPanel, 2 * kPanel, 0, kPanel}};   // -S^-1
     launch_small_gemm64_batch<F>(f, tb, 3, s, g);
     launch_small_gemm64<F>(f, TR, 2 * kPanel, Yb, kPanel, V11n, kPanel, TL, 2 * kPanel, true, s, g);
     g_launches += 6;
@@ -336,9 +338,10 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
   };
 
   // Chain of step t on the second stream: -P^-1 of the w x w block at (r, c)
-  // into Pn[t & 1]; a singular block records t in gbad. Its kernels are
-  // skipped once an earlier step has failed (Guard step t - 1). The host
-  // learns the result from h_bad[t & 1] after ev_inv[t & 1].
+  // into Pn[t & 1] and its limb planes into tBp[t & 1]; a singular block
+  // records t in gbad. Its kernels are skipped once an earlier step has
+  // failed (Guard step t - 1). The host learns the result from h_bad[t & 1]
+  // after ev_inv[t & 1].
   auto chain = [&](int t, int r, int c, int w) -> int {
     const Guard gc{gbad, t - 1};
     if (w == 2 * kPanel) {
@@ -348,27 +351,25 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
       g_launches++;
       CK(cudaGetLastError());
     }
+    CK(tc_split_b(*R.fp, Pn[t & 1], w, 0, w, w, tBp[t & 1], C->aux, gc));
+    g_launches++;
     CK(cudaMemcpyAsync(h_bad + (t & 1), gbad, sizeof(int), cudaMemcpyDeviceToHost, C->aux));
     CK(cudaEventRecord(C->ev_inv[t & 1], C->aux));
     return MODLIN_OK;
   };
 
   // W = P^-1 U[.., c1 .. c1+wn) = -(Pn U) into Wbuf (w rows, row stride n,
-  // columns c1 .. c1+wn), from 64 x 64 products accumulated over w / 64
-  // slices of the inner dimension.
+  // columns c1 .. c1+wn): one launch of (w / 64) x (wn / 64) products with
+  // inner dimension w.
   auto make_w = [&](const uint64_t* Pt, int r0, int w, int c1, int wn, const Guard& g) -> int {
-    for (int kb = 0; kb < w / kPanel; ++kb) {
-      SgProb pr[4];
-      int np = 0;
-      for (int i = 0; i < w / kPanel; ++i)
-        for (int j = 0; j < wn / kPanel; ++j) {
-          uint64_t* Cw = Wbuf + (int64_t)i * kPanel * n + c1 + j * kPanel;
-          pr[np++] = {Pt + (int64_t)i * kPanel * w + kb * kPanel, R.m + (int64_t)(r0 + kb * kPanel) * ld + c1 + j * kPanel,
-                      kb ? Cw : nullptr, Cw, w, ld, n, n, 1};
-        }
-      launch_small_gemm64_batch<F>(f, pr, np, st, g);
-      g_launches++;
-    }
+    SgProb pr[4];
+    int np = 0;
+    for (int i = 0; i < w / kPanel; ++i)
+      for (int j = 0; j < wn / kPanel; ++j)
+        pr[np++] = {Pt + (int64_t)i * kPanel * w, R.m + (int64_t)r0 * ld + c1 + j * kPanel, nullptr,
+                    Wbuf + (int64_t)i * kPanel * n + c1 + j * kPanel, w, ld, 0, n, 1, w};
+    launch_small_gemm64_batch<F>(f, pr, np, st, g);
+    g_launches++;
     return cuda_rc(cudaGetLastError());
   };
 
@@ -422,16 +423,15 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
         // w .. n - r0), as the wide update's A operand. Over 2^61 - 1 the
         // product writes H's limb planes directly; otherwise H goes through
         // Hb and a split.
-        CK(tc_split_b(*R.fp, Pt, w, 0, w, w, tBp, st, g));
         // With a chain running, one SM stays free for it (a CTA waiting for
         // that SM would hold up the whole product).
         const int ctas = wn > 0 ? C->num_sms - 1 : C->num_sms;
         if (fused) {
           const LimbOut lh{tA, w, w > kPanel ? 2 * kPanel : kPanel, 1};
-          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g, lh));
+          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp[t & 1], ctas, terr, st, g, lh));
         } else {
           launch_zero(Hb + (size_t)w * w, (int64_t)(n - r1) * w, st, g);
-          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp, ctas, terr, st, g));
+          CK(tc_update(*R.fp, Hb, w, w, n - r0, 0, w, w, tX[t & 1], tBp[t & 1], ctas, terr, st, g));
           CK(tc_split_a(*R.fp, Hb, w, 0, w, n - r0, w, tA, st, g));
           g_launches += 2;
         }
@@ -440,7 +440,7 @@ static int rank_impl(const RankRun& R, size_t* rank_out) {
         CK(tc_split_b(*R.fp, R.m + (int64_t)r0 * ld, ld, cw, n, w, tB, st, g));
         CK(tc_update(*R.fp, R.m, ld, r1, n, cw, n, w, tA, tB, ctas, terr, st, g));
         cudaEventRecord(evp.second, st);
-        g_launches += 4;
+        g_launches += 3;
       }
       // Step t's chain result (the GPU has step t queued meanwhile).
       CK(cudaEventSynchronize(C->ev_inv[t & 1]));

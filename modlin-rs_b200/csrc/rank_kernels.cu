@@ -768,7 +768,7 @@ struct SgBatch {
 };
 template <class F>
 __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
-  __shared__ uint64_t As[kSgTile][kPanel + 1], Bs[kPanel][kSgTile + 1];
+  __shared__ uint64_t As[kSgTile][2 * kPanel + 1], Bs[2 * kPanel][kSgTile + 1];
   pdl_wait();
   if (guard_skip(batch.g)) return;
   const SgProb& P = batch.p[blockIdx.x >> 4];
@@ -779,8 +779,8 @@ __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
     P.C[(int64_t)r * P.ldc + c] = P.D[(int64_t)r * P.ldd + c];
     return;
   }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  const int K = P.k == 2 * kPanel ? 2 * kPanel : kPanel;
+  for (int q = 0; q < K / 16; ++q) {
     const int kk = j + 16 * q;
     As[i][kk] = P.A[(int64_t)(ti * kSgTile + i) * P.lda + kk];
     Bs[i + 16 * q][j] = P.B[(int64_t)(i + 16 * q) * P.ldb + tj * kSgTile + j];
@@ -788,12 +788,12 @@ __global__ void __launch_bounds__(256) small_gemm64_kernel(F f, SgBatch batch) {
   __syncthreads();
   const uint64_t p = f.modulus(), sb = f.safe_batch();
   u128 acc = 0;
-  if (sb >= (uint64_t)kPanel) {
+  if (sb >= (uint64_t)K) {
 #pragma unroll 16
-    for (int k = 0; k < kPanel; ++k) acc += f.prod(As[i][k], Bs[k][j]);
+    for (int k = 0; k < K; ++k) acc += f.prod(As[i][k], Bs[k][j]);
   } else {
     uint64_t cnt = 0;
-    for (int k = 0; k < kPanel; ++k) {
+    for (int k = 0; k < K; ++k) {
       acc += f.prod(As[i][k], Bs[k][j]);
       if (++cnt == sb) {
         acc = f.reduce(acc);  // counts as one product from here on
@@ -909,7 +909,7 @@ void launch_small_gemm64_batch(const F& f, const SgProb* probs, int count, cudaS
 template <class F>
 void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint64_t* B, int64_t ldb, const uint64_t* D,
                          int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st, const Guard& g) {
-  const SgProb pr = {A, B, D, C, lda, ldb, ldd, ldc, negate ? 1 : 0};
+  const SgProb pr = {A, B, D, C, lda, ldb, ldd, ldc, negate ? 1 : 0, kPanel};
   launch_small_gemm64_batch<F>(f, &pr, 1, st, g);
 }
 

@@ -24,8 +24,8 @@ void launch_small_gemm64(const F& f, const uint64_t* A, int64_t lda, const uint6
                          int64_t ldd, uint64_t* C, int64_t ldc, bool negate, cudaStream_t st,
                          const Guard& g = Guard());
 // Up to kSgMaxProbs independent 64 x 64 products in one launch: problem i is
-// C = D - A * B (negate) or D + A * B (D may be null), or, with A null, the
-// copy C = D.
+// C = D - A * B (negate) or D + A * B (D may be null) with inner dimension k
+// (64 or 128; 0 means 64), or, with A null, the copy C = D.
 struct SgProb {
   const uint64_t* A;
   const uint64_t* B;
@@ -33,6 +33,7 @@ struct SgProb {
   uint64_t* C;
   int64_t lda, ldb, ldd, ldc;
   int negate;
+  int k;
 };
 constexpr int kSgMaxProbs = 4;
 template <class F>
