@@ -82,8 +82,8 @@ struct Shape {
   static constexpr int SMEM = A_BYTES + STAGES * B_BYTES + ZERO_BYTES + 1024 + C_BYTES;
   static_assert(SMEM <= 227 * 1024, "shared memory");
   // p = 2^61 - 1: the epilogue stages C by TMA, one 128 x 16 tile per group.
-  static constexpr int STAGES_M61 = KK == 64 ? 8 : 3;
-  static constexpr int C_TMA_BYTES = 2 * 128 * 16 * 8;  // one 128 x 16 C tile per epilogue group
+  static constexpr int STAGES_M61 = KK == 64 ? 8 : 2;
+  static constexpr int C_TMA_BYTES = 4 * 128 * 16 * 8;  // two 128 x 16 C tiles per epilogue group
   static constexpr int SMEM_M61 = A_BYTES + STAGES_M61 * B_BYTES + ZERO_BYTES + 1024 + C_TMA_BYTES;
   static_assert(SMEM_M61 <= 227 * 1024, "shared memory");
 };
@@ -286,8 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(acc_empty + b, kM61Path ? kEpiWarps / 2 : kEpiWarps);
     }
     mbar_init(mma_done, 1);
-    mbar_init(bars + 40, 1);  // c_full of epilogue group 0 (p = 2^61 - 1 with TMA)
-    mbar_init(bars + 41, 1);  // c_full of epilogue group 1
+    for (int q = 0; q < 4; ++q) mbar_init(bars + 40 + q, 1);  // c_full of (epilogue group, C buffer), 2^61 - 1
     for (int st = 0; st < kStages; ++st) {
       mbar_init(b_full + st, 1);
       mbar_init(b_empty + st, 1);
@@ -412,8 +411,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int row = quad * 32 + lane;
     const bool leader = (ew & 7) == 0 && lane == 0;
     const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + grp * 256 + half * 8;
-    uint64_t* cbuf = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024) + grp * (128 * 16);
-    uint64_t* c_full = bars + 40 + grp;
+    // Two C buffers per group: the tile of the group's next subtile loads
+    // while the current one is computed and stored.
+    uint64_t* cbuf0 = reinterpret_cast<uint64_t*>(sZ + SH::ZERO_BYTES + 1024) + grp * 2 * (128 * 16);
+    uint64_t* c_full0 = bars + 40 + 2 * grp;
     const int64_t nsub = S.nsub;
     // Subtile it = grp + 2 k of [g0, g1): (mt, sb) tracked incrementally.
     int64_t g = g0 + grp;
@@ -426,10 +427,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         ++mt;
       }
     };
-    int loads = 0;  // TMA loads issued by the leader (c_full phases)
+    int loads = 0;  // TMA loads issued by the leader; load j goes to buffer j & 1
     auto tma_load = [&]() {
-      mbar_arrive_expect_tx(c_full, 128 * 16 * 8);
-      tma_load_2d(cbuf, &cmap, (int32_t)(jend + sb * NS), (int32_t)(rbeg + mt * 128), c_full);
+      uint64_t* cf = c_full0 + (loads & 1);
+      mbar_arrive_expect_tx(cf, 128 * 16 * 8);
+      tma_load_2d(cbuf0 + (loads & 1) * (128 * 16), &cmap, (int32_t)(jend + sb * NS), (int32_t)(rbeg + mt * 128), cf);
       ++loads;
     };
     auto load_c = [&](uint64_t (&cv)[8]) {
@@ -454,10 +456,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     };
     uint64_t cv[8];
     if (g < g1 && !czero) {
-      if (!use_tma)
+      if (!use_tma) {
         load_c(cv);
-      else if (leader)
-        tma_load();
+      } else if (leader) {
+        tma_load();  // subtile 0 into buffer 0
+        if (g + 2 < g1) {
+          advance();
+          tma_load();  // subtile 1 into buffer 1
+          g -= 2;      // back to subtile 0
+          sb -= 2;
+          while (sb < 0) {
+            sb += nsub;
+            --mt;
+          }
+        }
+      }
     }
     bool ok = true;
     for (int k = 0; g < g1; ++k) {
@@ -480,7 +493,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       uint64_t res[8];
       if (tma) {
-        if (okw) okw = __all_sync(0xffffffffu, mbar_wait(c_full, k & 1, err));
+        uint64_t* const cbuf = cbuf0 + (k & 1) * (128 * 16);
+        if (okw) okw = __all_sync(0xffffffffu, mbar_wait(c_full0 + (k & 1), (k >> 1) & 1, err));
         if (okw) {
           // Row `row`, 16-byte chunks 4 half .. +4 of the 128-byte row; the
           // 128-byte swizzle XORs the chunk index (address bits 4-6) with
@@ -508,11 +522,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (leader) {
           tma_store_2d(&cmap, (int32_t)(jend + sb * NS), (int32_t)(rbeg + mt * 128), cbuf);
           bulk_commit();
-          bulk_wait_read0();  // the buffer is read; it can take the next tile
         }
         if (lo.Aw) put_limbs(res);
         advance();
-        if (leader && g < g1) tma_load();
+        if (leader && g < g1 && loads == k + 1) {
+          // The tile after next goes to the other buffer once the store
+          // issued from it one subtile ago has read it (this subtile's store
+          // may still be reading).
+          asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+          tma_load();
+        }
       } else {
         if (!okw) {
           ok = false;
@@ -535,7 +554,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (leader && tma) {
       bulk_wait_all0();  // stores complete
-      if (!ok && loads > 0) mbar_wait(c_full, (loads - 1) & 1, err + 1);  // a load still landing
+      if (!ok) {  // loads still landing: the last one into each buffer
+        for (int j = loads - 2 > 0 ? loads - 2 : 0; j < loads; ++j) mbar_wait(c_full0 + (j & 1), (j >> 1) & 1, err + 1);
+      }
     }
     if (!ok) atomicExch(err, 1);
   } else {
