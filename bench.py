@@ -185,6 +185,38 @@ def int8_peak_tops(torch):
         return None
 
 
+def int8_sustained_tops(torch, seconds=2.5):
+    """INT8 tensor throughput under the power cap: cuBLASLt int8 GEMMs
+    (8192^3, torch._int_mm) back to back for `seconds`, the last third timed
+    with CUDA events. The peak for a kernel timed inside a long step (the
+    burst figure above is for a kernel timed alone). None when unavailable."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t().contiguous().t()
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        while time.time() - t0 < seconds * 2 / 3:
+            for _ in range(8):
+                torch._int_mm(a, b)
+            torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = 0
+        s.record()
+        t1 = time.time()
+        while time.time() - t1 < seconds / 3:
+            for _ in range(8):
+                torch._int_mm(a, b)
+            n += 8
+            torch.cuda.synchronize()
+        e.record()
+        torch.cuda.synchronize()
+        del a, b
+        return 2 * 8192 ** 3 * n / (s.elapsed_time(e) * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
 def native_oracle():
     """The oracle built with -march=native for this host's CPU (the
     reference's release profile uses target-cpu=native), into a per-process
@@ -756,22 +788,30 @@ def prng_fill_measure(torch, modlin, count=1 << 32, host_sample=1 << 23, readme_
 
 
 def tc_update_schedule(n, two_panel_min):
-    """Trailing updates of a full-rank n x n rank on the tensor-core path:
-    two-panel steps (K = 128) while at least two_panel_min rows remain, then
-    one-panel steps (K = 64); returns (K = 128 updates, K = 64 updates, total
-    C outputs updated)."""
+    """Timed (wide) trailing updates of a full-rank n x n rank on the
+    tensor-core block pipeline: steps of w = 128 columns (K = 128) while at
+    least two_panel_min rows remain, then w = 64 (K = 64); each step's wide
+    update covers the rows below its block and the columns after the next
+    step's (the narrow update takes those). Returns (K = 128 updates, K = 64
+    updates, total C outputs of the wide updates)."""
+    def width(c):
+        if n - c >= two_panel_min and n - c >= 128:
+            return 128
+        return 64 if n - c >= 64 else 0
     col, k128, k64, outs = 0, 0, 0, 0
     while col < n:
-        if n - col >= two_panel_min and n - col >= 128:
-            if col + 128 < n:
+        w = width(col)
+        if w == 0:
+            break
+        wn = width(col + w) if col + w < n else 0
+        cw = col + w + wn
+        if col + w < n and cw < n:
+            if w == 128:
                 k128 += 1
-                outs += (n - col - 128) ** 2
-            col += 128
-        else:
-            if col + 64 < n:
+            else:
                 k64 += 1
-                outs += (n - col - 64) ** 2
-            col += 64
+            outs += (n - col - w) * (n - cw)
+        col += w
     return k128, k64, outs
 
 
@@ -1069,7 +1109,7 @@ def main():
         # measured u64 multiply-accumulate peak (the plain trailing update's
         # inner loop alone, all SMs); tensor-core work against the int8 GEMM.
         peak_int = extras["trailing_update"]["plain_mac_peak_modmac_per_s"]
-        int8 = int8_peak_tops(torch)
+        int8 = int8_sustained_tops(torch) or int8_peak_tops(torch)
         int_src = "measured: u64 x u64 -> u128 multiply-accumulate loop on operands in shared memory, all SMs " \
                   "(modlin_plain_mac_peak)"
         bm = extras["berlekamp_massey"]
@@ -1093,7 +1133,8 @@ def main():
         if int8:
             a = rp["tc"]["modmac_per_s"] * 128 / 1e12
             rp["roofline"] = {"bound": "tensor", "achieved": a, "peak": int8, "unit": "TFLOP/s", "frac": a / int8,
-                              "peak_source": "measured: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
+                              "peak_source": "measured, sustained: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) back to "
+                                             "back for 2.5 s on this GPU",
                               "note": "whole planted rank: all its modMACs x 64 limb products x 2 ops / rank time"}
 
     # End to end through the public C ABI with host buffers: pinned host
@@ -1160,7 +1201,13 @@ def main():
         per_launch_ms = tr_ms / max(n_tr, 1)
         if kernel == "tc":
             int8 = int8_peak_tops(torch)
-            if int8:
+            int8_s = int8_sustained_tops(torch)
+            if int8_s:
+                peak = int8_s
+                peak_note = ("measured, sustained: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) back to back for 2.5 s "
+                             "on this GPU (the wide updates run inside a long step under the power cap); burst "
+                             f"(best single GEMM): {int8:.0f} TOPS" if int8 else "")
+            elif int8:
                 peak, peak_note = int8, "measured: cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU"
             else:
                 peak = 2 * peaks.get("bf16_tflops", 1590.0)
@@ -1181,7 +1228,8 @@ def main():
                     "peak_source": peak_note,
                     "algorithmic_per_launch": f"{Wtr / max(n_tr, 1):.4g} modMAC x 64 limb products x 2 ops "
                                               f"({k128} updates at K = 128, {k64} at K = 64 per rank)",
-                    "avg_launch_ms": per_launch_ms}
+                    "avg_launch_ms": per_launch_ms,
+                    "peak_burst": int8, "frac_of_burst": achieved / int8 if int8 else None}
         else:
             peak = peaks.get("hbm_gbs", 6650.0)
             # Algorithmic bytes of the plain trailing update: C read + write.
